@@ -1,0 +1,205 @@
+"""Python binding of the prime-finder B200 engine (ctypes over the C ABI).
+
+The engine is the shared library ``prime-finder_b200/lib/libpfb200.so``
+built from ``prime-finder_b200/csrc`` (sm_100a CUDA + C ABI).  This module
+only marshals arguments; every computation runs in the library.  If the
+library is missing the import fails: there is no CPU fallback.
+
+Device buffers may be given as integers (raw device pointers) or as any
+object with ``data_ptr()`` (e.g. a CUDA ``torch.Tensor``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "lib", "libpfb200.so")
+
+PFB_OK = 0
+PFB_E_CUDA = -1
+PFB_E_ARG = -2
+PFB_E_NOMEM = -3
+PFB_E_CAPACITY = -4
+PFB_E_TIMEOUT = -5
+PFB_E_STATE = -6
+
+SIEVE_OR = 1
+SIEVE_MASK_HOST = 2
+SIEVE_MAX_K = 9999
+
+
+class PfbError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where} failed with code {code}: {last_error()}")
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load libpfb200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: run __graft_entry__.build() "
+                              "or `make -C prime-finder_b200/csrc`")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        u32p = C.POINTER(C.c_uint32)
+        ll = C.c_longlong
+        L.pfb_last_error.restype = C.c_char_p
+        L.pfb_sieve_mask_bytes.argtypes = [C.c_int]
+        L.pfb_sieve_mask_bytes.restype = C.c_size_t
+        L.pfb_sieve_create.argtypes = [C.POINTER(vp), u32p, C.c_uint32, C.c_int]
+        L.pfb_sieve_create.restype = C.c_int
+        L.pfb_sieve_destroy.argtypes = [vp]
+        L.pfb_sieve_destroy.restype = None
+        L.pfb_sieve_run.argtypes = [vp, C.POINTER(ll), C.c_int, C.c_int, vp, C.c_uint, vp]
+        L.pfb_sieve_run.restype = C.c_int
+        L.pfb_sieve_survivors.argtypes = [vp, vp, C.c_int, vp, C.c_uint32, u32p, vp]
+        L.pfb_sieve_survivors.restype = C.c_int
+        L.trial_div_gpu_grid.argtypes = [u32p, C.c_uint32, C.POINTER(ll), C.c_int, C.c_int,
+                                         vp, C.c_uint]
+        L.trial_div_gpu_grid.restype = C.c_int
+        L.trial_div_gpu.argtypes = [vp, ll, ll, ll, u32p, vp]
+        L.trial_div_gpu.restype = C.c_int
+        L.cuda_get_device_count.restype = C.c_int
+        L.cuda_set_device.argtypes = [C.c_int]
+        L.cuda_set_device.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    if _lib is None:
+        return ""
+    s = _lib.pfb_last_error()
+    return s.decode() if s else ""
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != PFB_OK:
+        raise PfbError(rc, where)
+
+
+def _dptr(x) -> int:
+    if x is None:
+        return 0
+    if isinstance(x, int):
+        return x
+    return int(x.data_ptr())
+
+
+def _u32(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_uint32))
+
+
+def _abc_array(abc: Sequence[Tuple[int, int, int]]):
+    flat = np.ascontiguousarray(np.asarray(abc, dtype=np.int64).reshape(-1))
+    return flat, flat.ctypes.data_as(C.POINTER(C.c_longlong)), len(flat) // 3
+
+
+# ------------------------------------------------------------------ sieve ---
+
+def mask_bytes(K: int) -> int:
+    return int(lib().pfb_sieve_mask_bytes(K))
+
+
+class PrimeList(C.Structure):
+    """prime_list_t (prime_list.h): { uint32_t *primes; uint32_t count; }"""
+    _fields_ = [("primes", C.POINTER(C.c_uint32)), ("count", C.c_uint32)]
+
+
+class GpuTiming(C.Structure):
+    """gpu_timing_t (trial_div.h): upload / kernel / download seconds."""
+    _fields_ = [("upload", C.c_double), ("kernel", C.c_double), ("download", C.c_double)]
+
+
+def trial_div_gpu(primes: np.ndarray, a: int, b: int, c: int,
+                  sieve_bits: Optional[np.ndarray] = None,
+                  timing: Optional[GpuTiming] = None) -> np.ndarray:
+    """Drop-in ``trial_div_gpu`` (100 x 100 grid, 313 uint32 words, OR-in)."""
+    primes = np.ascontiguousarray(primes, dtype=np.uint32)
+    if sieve_bits is None:
+        sieve_bits = np.zeros(313, dtype=np.uint32)
+    assert sieve_bits.dtype == np.uint32 and sieve_bits.size >= 313
+    pl = PrimeList(_u32(primes), len(primes))
+    rc = lib().trial_div_gpu(C.addressof(pl), a, b, c, _u32(sieve_bits),
+                             C.addressof(timing) if timing is not None else None)
+    if rc != 0:
+        raise PfbError(rc, "trial_div_gpu")
+    return sieve_bits
+
+
+def trial_div_gpu_grid(primes: np.ndarray, abc, K: int,
+                       mask: Optional[np.ndarray] = None, or_in: bool = False) -> np.ndarray:
+    """Stateless wide-grid sieve with host buffers; returns the packed masks."""
+    primes = np.ascontiguousarray(primes, dtype=np.uint32)
+    flat, pabc, n = _abc_array(abc)
+    blk = mask_bytes(K)
+    if mask is None:
+        mask = np.zeros(blk * n, dtype=np.uint8)
+    assert mask.nbytes >= blk * n and mask.flags.c_contiguous
+    rc = lib().trial_div_gpu_grid(_u32(primes), len(primes), pabc, n, K,
+                                  mask.ctypes.data, SIEVE_OR if or_in else 0)
+    _check(rc, "trial_div_gpu_grid")
+    return mask
+
+
+class Sieve:
+    """A sieve context: the prime list resident in device memory."""
+
+    def __init__(self, primes: np.ndarray, device: int = 0):
+        primes = np.ascontiguousarray(primes, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(lib().pfb_sieve_create(C.byref(h), _u32(primes), len(primes), device),
+               "pfb_sieve_create")
+        self._h = h
+        self.device = device
+        self.n_primes = len(primes)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().pfb_sieve_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, abc, K: int, mask=None, or_in: bool = False, stream: int = 0):
+        """Sieve triples into ``mask``: a host ``np.uint8`` array (synchronous) or
+        a device buffer (asynchronous on ``stream``).  Returns the mask."""
+        flat, pabc, n = _abc_array(abc)
+        flags = SIEVE_OR if or_in else 0
+        if mask is None or isinstance(mask, np.ndarray):
+            if mask is None:
+                mask = np.zeros(mask_bytes(K) * n, dtype=np.uint8)
+            assert mask.nbytes >= mask_bytes(K) * n
+            rc = lib().pfb_sieve_run(self._h, pabc, n, K, mask.ctypes.data,
+                                     flags | SIEVE_MASK_HOST, stream or None)
+        else:
+            rc = lib().pfb_sieve_run(self._h, pabc, n, K, _dptr(mask), flags, stream or None)
+        _check(rc, "pfb_sieve_run")
+        return mask
+
+    def survivors(self, d_mask, K: int, d_out, cap: int, stream: int = 0) -> int:
+        cnt = C.c_uint32(0)
+        rc = lib().pfb_sieve_survivors(self._h, _dptr(d_mask), K, _dptr(d_out), cap,
+                                       C.byref(cnt), stream or None)
+        if rc not in (PFB_OK, PFB_E_CAPACITY):
+            _check(rc, "pfb_sieve_survivors")
+        return int(cnt.value)
+
+
+def unpack_mask(mask: np.ndarray, K: int) -> np.ndarray:
+    """Packed mask block -> bool array [K, K] (True = eliminated)."""
+    bits = np.unpackbits(np.asarray(mask, dtype=np.uint8)[: (K * K + 7) // 8], bitorder="little")
+    return bits[: K * K].reshape(K, K).astype(bool)

@@ -1,0 +1,57 @@
+"""The C-ABI library loads and exports every function include/*.h declares.
+
+No GPU needed: this only opens libpfb200.so and resolves symbols.
+"""
+import ctypes
+import os
+import re
+
+import pfb200
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+INC = os.path.join(ROOT, "include")
+
+# C++-linkage helpers (declared outside extern "C") are matched by substring.
+_CPP_LINKAGE = {"trial_div_launch"}
+
+
+def _declared_functions():
+    names = set()
+    for fn in sorted(os.listdir(INC)):
+        if not fn.endswith(".h"):
+            continue
+        src = open(os.path.join(INC, fn)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"//[^\n]*", "", src)
+        src = re.sub(r"#[^\n]*", "", src)
+        src = re.sub(r"typedef[^;]*;", "", src)
+        for m in re.finditer(r"([A-Za-z_][A-Za-z0-9_]*)\s*\(([^;{}]*)\)\s*;", src):
+            name = m.group(1)
+            if name in ("if", "while", "for", "return", "sizeof"):
+                continue
+            names.add(name)
+    return names
+
+
+def test_library_loads():
+    L = pfb200.lib()
+    assert pfb200.mask_bytes(100) == 313 * 4
+    assert pfb200.mask_bytes(9999) == ((9999 * 9999 + 31) // 32) * 4
+
+
+def test_every_declared_symbol_is_exported():
+    L = pfb200.lib()
+    declared = _declared_functions()
+    assert "trial_div_gpu" in declared and "pfb_sieve_run" in declared
+    missing = []
+    for name in sorted(declared):
+        if name in _CPP_LINKAGE:
+            out = os.popen(f"nm -D --defined-only {pfb200.LIB_PATH}").read()
+            if name not in out:
+                missing.append(name)
+            continue
+        try:
+            getattr(L, name)
+        except AttributeError:
+            missing.append(name)
+    assert not missing, missing
