@@ -1,0 +1,233 @@
+// Host-side multi-precision helpers for the Miller-Rabin set-up.
+//
+// The reference does this set-up with GMP on the host (Barrett's mu,
+// barrett.cu:29-107; Montgomery's N', montgomery.cu:30-45; residues of the
+// witness, miller_rabin_runner.cu:315-325).  This engine needs, per modulus
+// N and Montgomery radix R = 2^(22*H):
+//   * N' = -N^-1 mod R                 (Hensel lifting)
+//   * R mod N                          (Knuth's long division, TAOCP 4.3.1 D)
+//   * N - 1 = 2^s * d                  (bit scan)
+// Numbers are little-endian vectors of 64-bit words.
+#pragma once
+#include <stdint.h>
+
+#include <algorithm>
+#include <vector>
+
+namespace pfb {
+namespace big {
+
+using Words = std::vector<uint64_t>;
+
+inline void trim(Words &a) {
+    while (!a.empty() && a.back() == 0) a.pop_back();
+}
+
+inline size_t bit_length(const Words &a) {
+    for (size_t i = a.size(); i-- > 0;)
+        if (a[i]) return i * 64 + (64 - __builtin_clzll(a[i]));
+    return 0;
+}
+
+inline bool test_bit(const Words &a, size_t i) {
+    return (i / 64 < a.size()) && ((a[i / 64] >> (i % 64)) & 1ull);
+}
+
+inline Words from_u16(const uint16_t *l, size_t n) {
+    Words w((n + 3) / 4, 0);
+    for (size_t i = 0; i < n; i++) w[i / 4] |= (uint64_t)l[i] << (16 * (i % 4));
+    trim(w);
+    return w;
+}
+
+inline void to_u16(const Words &a, uint16_t *out, size_t n) {
+    for (size_t i = 0; i < n; i++) out[i] = (i / 4 < a.size()) ? (uint16_t)(a[i / 4] >> (16 * (i % 4))) : 0;
+}
+
+// Little-endian `bits`-bit limbs (bits <= 32), exactly n of them.
+inline void to_limbs(const Words &a, unsigned bits, uint32_t *out, size_t n) {
+    const uint64_t mask = (1ull << bits) - 1ull;
+    for (size_t i = 0; i < n; i++) {
+        const size_t bit = i * bits, wi = bit / 64, sh = bit % 64;
+        uint64_t v = 0;
+        if (wi < a.size()) {
+            v = a[wi] >> sh;
+            if (sh + bits > 64 && wi + 1 < a.size()) v |= a[wi + 1] << (64 - sh);
+        }
+        out[i] = (uint32_t)(v & mask);
+    }
+}
+
+inline Words from_limbs(const uint32_t *l, unsigned bits, size_t n) {
+    Words w((n * bits + 63) / 64 + 1, 0);
+    for (size_t i = 0; i < n; i++) {
+        const size_t bit = i * bits, wi = bit / 64, sh = bit % 64;
+        w[wi] |= (uint64_t)l[i] << sh;
+        if (sh + bits > 64) w[wi + 1] |= (uint64_t)l[i] >> (64 - sh);
+    }
+    trim(w);
+    return w;
+}
+
+inline int cmp(const Words &a, const Words &b) {
+    if (a.size() != b.size()) return a.size() < b.size() ? -1 : 1;
+    for (size_t i = a.size(); i-- > 0;)
+        if (a[i] != b[i]) return a[i] < b[i] ? -1 : 1;
+    return 0;
+}
+
+inline Words sub_small(Words a, uint64_t s) {
+    for (size_t i = 0; i < a.size() && s; i++) {
+        const uint64_t v = a[i];
+        a[i] = v - s;
+        s = (v < s) ? 1 : 0;
+    }
+    trim(a);
+    return a;
+}
+
+inline Words shr(const Words &a, size_t s) {
+    const size_t ws = s / 64, bs = s % 64;
+    if (ws >= a.size()) return Words();
+    Words r(a.size() - ws, 0);
+    for (size_t i = 0; i < r.size(); i++) {
+        uint64_t v = a[i + ws] >> bs;
+        if (bs && i + ws + 1 < a.size()) v |= a[i + ws + 1] << (64 - bs);
+        r[i] = v;
+    }
+    trim(r);
+    return r;
+}
+
+// (a * b) mod 2^(64*k), schoolbook, truncated.
+inline Words mullo(const Words &a, const Words &b, size_t k) {
+    Words r(k, 0);
+    for (size_t i = 0; i < a.size() && i < k; i++) {
+        unsigned __int128 carry = 0;
+        const uint64_t ai = a[i];
+        if (!ai) continue;
+        for (size_t j = 0; j < b.size() && i + j < k; j++) {
+            unsigned __int128 t = (unsigned __int128)ai * b[j] + r[i + j] + carry;
+            r[i + j] = (uint64_t)t;
+            carry = t >> 64;
+        }
+        for (size_t j = i + b.size(); j < k && carry; j++) {
+            unsigned __int128 t = (unsigned __int128)r[j] + carry;
+            r[j] = (uint64_t)t;
+            carry = t >> 64;
+        }
+    }
+    return r;
+}
+
+// -N^-1 mod 2^bits for odd N (Hensel / Newton: x <- x*(2 - N*x)).
+inline Words neg_inv_pow2(const Words &N, size_t bits) {
+    uint64_t x0 = N[0];  // N*N == 1 mod 8 for odd N
+    for (int i = 0; i < 6; i++) x0 *= 2 - N[0] * x0;
+    Words x(1, x0);
+    size_t k = 1;
+    const size_t kmax = (bits + 63) / 64;
+    while (k < kmax) {
+        k = std::min(2 * k, kmax);
+        Words nx = mullo(N, x, k);           // N*x = 1 + e
+        // 2 - N*x  (mod 2^(64k))
+        Words t(k, 0);
+        unsigned __int128 borrow = 0;
+        for (size_t i = 0; i < k; i++) {
+            const uint64_t two = (i == 0) ? 2 : 0;
+            const uint64_t v = (i < nx.size()) ? nx[i] : 0;
+            unsigned __int128 d = (unsigned __int128)two - v - (uint64_t)borrow;
+            t[i] = (uint64_t)d;
+            borrow = (d >> 64) ? 1 : 0;
+        }
+        x = mullo(x, t, k);
+    }
+    // negate mod 2^(64*kmax), then truncate to `bits`
+    Words r(kmax, 0);
+    unsigned __int128 carry = 1;
+    for (size_t i = 0; i < kmax; i++) {
+        unsigned __int128 v = (unsigned __int128)(uint64_t)(~(i < x.size() ? x[i] : 0ull)) + carry;
+        r[i] = (uint64_t)v;
+        carry = v >> 64;
+    }
+    if (bits % 64) r[kmax - 1] &= (1ull << (bits % 64)) - 1ull;
+    trim(r);
+    return r;
+}
+
+// 2^e mod N by Knuth's algorithm D on 32-bit digits (N > 1).
+inline Words pow2_mod(size_t e, const Words &N) {
+    // digits of N
+    std::vector<uint32_t> v;
+    for (uint64_t w : N) {
+        v.push_back((uint32_t)w);
+        v.push_back((uint32_t)(w >> 32));
+    }
+    while (!v.empty() && v.back() == 0) v.pop_back();
+    const size_t n = v.size();
+    // u = 2^e as digits
+    std::vector<uint32_t> u(e / 32 + 1, 0);
+    u[e / 32] = 1u << (e % 32);
+    if (n == 1) {
+        uint64_t r = 0;
+        for (size_t i = u.size(); i-- > 0;) r = ((r << 32) | u[i]) % v[0];
+        return Words(1, r);
+    }
+    if (u.size() < n) {  // 2^e < N
+        Words r((u.size() + 1) / 2, 0);
+        for (size_t i = 0; i < u.size(); i++) r[i / 2] |= (uint64_t)u[i] << (32 * (i % 2));
+        trim(r);
+        return r;
+    }
+    const int s = __builtin_clz(v[n - 1]);
+    std::vector<uint32_t> vn(n), un(u.size() + 1);
+    for (size_t i = n - 1; i > 0; i--) vn[i] = (v[i] << s) | (s ? (uint32_t)((uint64_t)v[i - 1] >> (32 - s)) : 0u);
+    vn[0] = v[0] << s;
+    const size_t m = u.size() - n;
+    un[u.size()] = s ? (uint32_t)((uint64_t)u[u.size() - 1] >> (32 - s)) : 0u;
+    for (size_t i = u.size() - 1; i > 0; i--) un[i] = (u[i] << s) | (s ? (uint32_t)((uint64_t)u[i - 1] >> (32 - s)) : 0u);
+    un[0] = u[0] << s;
+    const uint64_t b = 1ull << 32;
+    for (size_t jj = m + 1; jj-- > 0;) {
+        const size_t j = jj;
+        uint64_t num = ((uint64_t)un[j + n] << 32) | un[j + n - 1];
+        uint64_t qhat = num / vn[n - 1];
+        uint64_t rhat = num - qhat * vn[n - 1];
+        while (qhat >= b || qhat * vn[n - 2] > ((rhat << 32) | un[j + n - 2])) {
+            qhat--;
+            rhat += vn[n - 1];
+            if (rhat >= b) break;
+        }
+        int64_t borrow = 0;
+        uint64_t carry = 0;
+        for (size_t i = 0; i < n; i++) {
+            const uint64_t p = qhat * vn[i] + carry;
+            carry = p >> 32;
+            const int64_t t = (int64_t)un[i + j] - (int64_t)(uint32_t)p - borrow;
+            un[i + j] = (uint32_t)t;
+            borrow = (t < 0) ? 1 : 0;
+        }
+        const int64_t t = (int64_t)un[j + n] - (int64_t)carry - borrow;
+        un[j + n] = (uint32_t)t;
+        if (t < 0) {  // add back
+            uint64_t c = 0;
+            for (size_t i = 0; i < n; i++) {
+                const uint64_t sum = (uint64_t)un[i + j] + vn[i] + c;
+                un[i + j] = (uint32_t)sum;
+                c = sum >> 32;
+            }
+            un[j + n] += (uint32_t)c;
+        }
+    }
+    // remainder = un[0..n) >> s
+    std::vector<uint32_t> r(n);
+    for (size_t i = 0; i < n; i++)
+        r[i] = (un[i] >> s) | (s ? (uint32_t)((uint64_t)un[i + 1] << (32 - s)) : 0u);
+    Words out((n + 1) / 2, 0);
+    for (size_t i = 0; i < n; i++) out[i / 2] |= (uint64_t)r[i] << (32 * (i % 2));
+    trim(out);
+    return out;
+}
+
+}  // namespace big
+}  // namespace pfb

@@ -1,0 +1,366 @@
+// Device arithmetic of the Miller-Rabin engine: one CTA owns one candidate and
+// runs whole Montgomery squarings on chip.
+//
+// Replaces the reference's per-squaring chain of ~39 launches
+// (batch_mod_ctx.cu:288-316 -> ntt_4step.cu:202-295 -> carry_norm.cu:63-122
+// -> barrett.cu:128-199 / sub.cu:18-155) with one CTA-resident sequence:
+//
+//   x (H limbs of 22 bits, x < 4N)          R = 2^(22*H), L = 2H
+//   T  = x^2                  cyclic NTT of length L over p1 and p2, CRT
+//   m  = (T mod R) * N' mod R length-L NTT product with the stored NTT(N')
+//   W  = m * N mod (R - 1)    length-H cyclic NTT product with the stored NTT(N)
+//   U  = (T_lo + T_hi + W) mod (R - 1)
+//
+// U equals (T + m N) / R (Montgomery's REDC): T + mN == 0 (mod R), and
+// modulo R - 1 the quotient by R is the sum of the halves; 0 <= U < 2N < R-1
+// makes the residue exact.  Exact 30-bit modular butterflies (Shoup's
+// multiplication, Harvey's lazy [0, 2p) ranges) run on the integer pipe.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfb {
+namespace mr {
+
+constexpr uint32_t P1 = 998244353u;   // 119 * 2^23 + 1, primitive root 3
+constexpr uint32_t P2 = 1004535809u;  // 479 * 2^21 + 1, primitive root 3
+constexpr int LIMB_BITS = 22;
+constexpr uint32_t LIMB_MASK = (1u << LIMB_BITS) - 1u;
+constexpr int LOG_LMAX = 15;          // twiddle tables cover L <= 2^15
+constexpr int LOG_LMIN = 8;
+constexpr int LOG_LCTA = 14;          // largest L whose two transforms fit one CTA
+constexpr int THREADS = 512;
+
+// Twiddles: w[p][k] = omega^k, omega of order 2^LOG_LMAX, k < 2^(LOG_LMAX-1);
+// wi = omega^-k.  *_sh are Shoup companions floor(w * 2^32 / p).
+struct Twiddles {
+    const uint32_t *w[2], *wsh[2], *wi[2], *wish[2];
+};
+
+// Per transform length (index logn): sigma = 2^32 / n mod p (undoes the
+// Montgomery factor of the pointwise product and the 1/n of the inverse).
+struct CrtConsts {
+    uint32_t s1[LOG_LMAX + 1], s1sh[LOG_LMAX + 1];   // sigma mod p1
+    uint32_t k2[LOG_LMAX + 1], k2sh[LOG_LMAX + 1];   // sigma * p1^-1 mod p2
+    uint32_t k1, k1sh;                               // p1^-1 mod p2
+    uint32_t pinv[2];                                // -p^-1 mod 2^32
+};
+
+__device__ __forceinline__ int pad(int i) { return i + (i >> 5); }
+
+__device__ __forceinline__ uint32_t shoup(uint32_t a, uint32_t w, uint32_t wsh, uint32_t p) {
+    const uint32_t q = __umulhi(a, wsh);
+    return a * w - q * p;  // in [0, 2p) for a < 2^32
+}
+
+__device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b, uint32_t p, uint32_t pinv) {
+    const uint32_t lo = a * b, hi = __umulhi(a, b);
+    const uint32_t m = lo * pinv;
+    return hi + __umulhi(m, p) + (lo != 0u);  // in [0, 2p) for a, b < 2p
+}
+
+__device__ __forceinline__ uint32_t red2(uint32_t x, uint32_t p2) { return x >= p2 ? x - p2 : x; }
+
+// Radix-2^RLOG decimation-in-frequency pass over both primes (natural order in,
+// bit-reversed out after all passes).  h0 = half size of the first stage.
+template <int RLOG>
+__device__ __forceinline__ void dif_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
+    constexpr int R = 1 << RLOG;
+    const int groups = (1 << logn) >> RLOG;
+    const int sub = (2 * h0) >> RLOG;  // element stride inside a group
+    const int lh0 = 31 - __clz(h0);
+    for (int g = threadIdx.x; g < 2 * groups; g += blockDim.x) {
+        const int pr = g >= groups;
+        const int gg = g - (pr ? groups : 0);
+        uint32_t *A = pr ? A1 : A0;
+        const uint32_t p = pr ? P2 : P1, p2 = 2u * p;
+        const uint32_t *W = tw.w[pr], *Wsh = tw.wsh[pr];
+        const int block = gg / sub, j0 = gg - block * sub;
+        const int base = block * 2 * h0 + j0;
+        uint32_t v[R];
+#pragma unroll
+        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * sub)];
+#pragma unroll
+        for (int s = 0; s < RLOG; s++) {
+            const int half = R >> (s + 1);
+            const int shift = LOG_LMAX - 1 - (lh0 - s);  // k = j << shift
+#pragma unroll
+            for (int e = 0; e < R; e++) {
+                if (e & half) continue;
+                const int j = j0 + (e & (half - 1)) * sub;
+                const int k = j << shift;
+                const uint32_t x = v[e], y = v[e + half];
+                v[e] = red2(x + y, p2);
+                v[e + half] = shoup(x - y + p2, __ldg(W + k), __ldg(Wsh + k), p);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < R; e++) A[pad(base + e * sub)] = v[e];
+    }
+}
+
+// Radix-2^RLOG decimation-in-time pass (bit-reversed in, natural out); h0 =
+// half size of the first (smallest) stage.
+template <int RLOG>
+__device__ __forceinline__ void dit_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
+    constexpr int R = 1 << RLOG;
+    const int groups = (1 << logn) >> RLOG;
+    const int lh0 = 31 - __clz(h0);
+    for (int g = threadIdx.x; g < 2 * groups; g += blockDim.x) {
+        const int pr = g >= groups;
+        const int gg = g - (pr ? groups : 0);
+        uint32_t *A = pr ? A1 : A0;
+        const uint32_t p = pr ? P2 : P1, p2 = 2u * p;
+        const uint32_t *W = tw.wi[pr], *Wsh = tw.wish[pr];
+        const int block = gg >> lh0, j0 = gg & (h0 - 1);
+        const int base = block * R * h0 + j0;
+        uint32_t v[R];
+#pragma unroll
+        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * h0)];
+#pragma unroll
+        for (int s = 0; s < RLOG; s++) {
+            const int half = 1 << s;
+            const int shift = LOG_LMAX - 1 - (lh0 + s);
+#pragma unroll
+            for (int e = 0; e < R; e++) {
+                if (e & half) continue;
+                const int j = j0 + (e & (half - 1)) * h0;
+                const int k = j << shift;
+                const uint32_t x = v[e];
+                const uint32_t t = shoup(v[e + half], __ldg(W + k), __ldg(Wsh + k), p);
+                v[e] = red2(x + t, p2);
+                v[e + half] = red2(x - t + p2, p2);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < R; e++) A[pad(base + e * h0)] = v[e];
+    }
+}
+
+__device__ void dif(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
+    int s = logn, h0 = 1 << (logn - 1);
+    while (s > 0) {
+        if (s >= 4) {
+            dif_pass<4>(A0, A1, logn, h0, tw);
+            h0 >>= 4;
+            s -= 4;
+        } else if (s == 3) {
+            dif_pass<3>(A0, A1, logn, h0, tw);
+            s = 0;
+        } else if (s == 2) {
+            dif_pass<2>(A0, A1, logn, h0, tw);
+            s = 0;
+        } else {
+            dif_pass<1>(A0, A1, logn, h0, tw);
+            s = 0;
+        }
+        __syncthreads();
+    }
+}
+
+__device__ void dit(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
+    int s = logn, h0 = 1;
+    const int r0 = logn & 3;  // remainder pass first
+    if (r0) {
+        if (r0 == 3) dit_pass<3>(A0, A1, logn, h0, tw);
+        else if (r0 == 2) dit_pass<2>(A0, A1, logn, h0, tw);
+        else dit_pass<1>(A0, A1, logn, h0, tw);
+        h0 <<= r0;
+        s -= r0;
+        __syncthreads();
+    }
+    while (s > 0) {
+        dit_pass<4>(A0, A1, logn, h0, tw);
+        h0 <<= 4;
+        s -= 4;
+        __syncthreads();
+    }
+}
+
+// Scratch of the carry-lookahead scan.
+struct CarrySmem {
+    unsigned long long wc[THREADS / 32];
+    uint32_t wg[THREADS / 32], wp[THREADS / 32], wcin[THREADS / 32];
+    unsigned long long total;
+    unsigned long long aux[4];
+};
+
+// Turns n raw coefficients get(i) (each < 2^63 - 2^42) plus a carry cin0 at
+// position 0 into n limbs of 22 bits written to out[] (padded index when
+// PAD), and returns the carry out of position n-1.  Each thread propagates a
+// segment of n/T consecutive positions; the carries between segments are
+// resolved by a generate/propagate scan (warp ballots, then across warps).
+template <bool PAD, class Get>
+__device__ unsigned long long carry_pass(const int n, const unsigned long long cin0, Get get, uint32_t *out,
+                                         CarrySmem &cs) {
+    const int T = blockDim.x;
+    const int w = n >= T ? n / T : 1;
+    const int na = n / w;
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const unsigned FULL = 0xffffffffu;
+    unsigned long long acc = 0, room = ~0ull;
+    if (t < na) {
+        const int lo = t * w;
+        uint32_t l0 = 0, l1 = 0;
+        bool ones = true;
+        for (int q = 0; q < w; q++) {
+            acc += get(lo + q);
+            const uint32_t limb = (uint32_t)acc & LIMB_MASK;
+            acc >>= LIMB_BITS;
+            out[PAD ? pad(lo + q) : lo + q] = limb;
+            if (q == 0) l0 = limb;
+            else if (q == 1) l1 = limb;
+            else ones = ones && (limb == LIMB_MASK);
+        }
+        if (w == 1) room = (1ull << LIMB_BITS) - l0;
+        else if (ones) room = (1ull << (2 * LIMB_BITS)) - ((unsigned long long)l1 << LIMB_BITS) - l0;
+    }
+    unsigned long long prev = __shfl_up_sync(FULL, acc, 1);
+    if (lane == 31) cs.wc[warp] = acc;
+    __syncthreads();
+    if (lane == 0) prev = (warp == 0) ? cin0 : cs.wc[warp - 1];
+    const bool G = (t < na) && (prev >= room);
+    const bool Pr = (t < na) && !G && (prev + 1ull == room);
+    const uint32_t g = __ballot_sync(FULL, G), p = __ballot_sync(FULL, Pr);
+    const unsigned long long gp = (unsigned long long)(g | p);
+    if (lane == 0) {
+        const uint32_t o0 = (uint32_t)(((unsigned long long)g + gp) >> 32);
+        const uint32_t o1 = (uint32_t)(((unsigned long long)g + gp + 1ull) >> 32);
+        cs.wg[warp] = o0;
+        cs.wp[warp] = o1 & (o0 ^ 1u);
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int nw = (T + 31) >> 5;
+        const uint32_t G2 = __ballot_sync(FULL, lane < nw && cs.wg[lane]);
+        const uint32_t P2m = __ballot_sync(FULL, lane < nw && cs.wp[lane]);
+        const uint32_t X2 = (uint32_t)((unsigned long long)G2 + (unsigned long long)(G2 | P2m));
+        const uint32_t cinw = X2 ^ P2m;
+        if (lane < nw) cs.wcin[lane] = (cinw >> lane) & 1u;
+    }
+    __syncthreads();
+    const uint32_t X = (uint32_t)((unsigned long long)g + gp + cs.wcin[warp]);
+    const uint32_t dprev = ((X ^ p) >> lane) & 1u;
+    const unsigned long long cin = prev + dprev;
+    if (t < na && cin) {
+        const int lo = t * w;
+        unsigned long long a2 = cin;
+        for (int q = 0; q < w && a2; q++) {
+            const int ix = PAD ? pad(lo + q) : lo + q;
+            a2 += out[ix];
+            out[ix] = (uint32_t)a2 & LIMB_MASK;
+            a2 >>= LIMB_BITS;
+        }
+    }
+    if (t == na - 1) cs.total = acc + ((G || (Pr && dprev)) ? 1ull : 0ull);
+    __syncthreads();
+    const unsigned long long tot = cs.total;
+    __syncthreads();
+    return tot;
+}
+
+__device__ __forceinline__ unsigned long long crt(uint32_t r1, uint32_t r2, int logn, const CrtConsts &cc) {
+    uint32_t c1 = shoup(r1, cc.s1[logn], cc.s1sh[logn], P1);
+    c1 = red2(c1, P1);
+    const uint32_t a = shoup(r2, cc.k2[logn], cc.k2sh[logn], P2);
+    const uint32_t b = shoup(c1, cc.k1, cc.k1sh, P2);
+    uint32_t t = a + 2u * P2 - b;  // (0, 4 p2)
+    t = red2(t, 2u * P2);
+    t = red2(t, P2);
+    return (unsigned long long)c1 + (unsigned long long)P1 * t;
+}
+
+// Per-CTA view of one candidate.
+struct Cand {
+    const uint32_t *nph;   // NTT_L(N')  [2][L] (bit-reversed spectral order)
+    const uint32_t *nh;    // NTT_H(N)   [2][H]
+    int logl;
+};
+
+struct Smem {
+    uint32_t *A0, *A1, *X;
+    CarrySmem *cs;
+};
+
+// One Montgomery step on X (H limbs): X <- REDC(X^2) * a   (square = true)
+//                                   or X <- REDC(X)           (square = false).
+// On entry X < 4N (or < R for square = false); on exit X < 2N * a.
+__device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
+                          const CrtConsts &cc) {
+    const int logl = cd.logl, L = 1 << logl, H = L >> 1;
+    uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
+    CarrySmem &cs = *sm.cs;
+    const int tid = threadIdx.x, T = blockDim.x;
+    unsigned long long cS = 0;  // carry of T_lo + T_hi
+
+    if (square) {
+        for (int i = tid; i < L; i += T) {
+            const uint32_t v = i < H ? X[i] : 0u;
+            A0[pad(i)] = v;
+            A1[pad(i)] = v;
+        }
+        __syncthreads();
+        dif(A0, A1, logl, tw);
+        for (int i = tid; i < L; i += T) {
+            const int q = pad(i);
+            const uint32_t u = A0[q], v = A1[q];
+            A0[q] = mont(u, u, P1, cc.pinv[0]);
+            A1[q] = mont(v, v, P2, cc.pinv[1]);
+        }
+        __syncthreads();
+        dit(A0, A1, logl, tw);
+        // T = x^2 as L limbs, in place over A0
+        carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
+        // S1 = T_lo + T_hi  -> X, carry cS
+        cS = carry_pass<false>(H, 0ull,
+                               [&](int i) { return (unsigned long long)A0[pad(i)] + A0[pad(i + H)]; }, X, cs);
+        for (int i = tid; i < L; i += T) {
+            const int q = pad(i);
+            if (i < H) A1[q] = A0[q];
+            else A0[q] = A1[q] = 0u;
+        }
+        __syncthreads();
+    } else {
+        for (int i = tid; i < L; i += T) {
+            const uint32_t v = i < H ? X[i] : 0u;
+            A0[pad(i)] = v;
+            A1[pad(i)] = v;
+        }
+        __syncthreads();
+    }
+    // m = T_lo * N' mod R
+    dif(A0, A1, logl, tw);
+    for (int i = tid; i < L; i += T) {
+        const int q = pad(i);
+        A0[q] = mont(A0[q], __ldg(cd.nph + i), P1, cc.pinv[0]);
+        A1[q] = mont(A1[q], __ldg(cd.nph + L + i), P2, cc.pinv[1]);
+    }
+    __syncthreads();
+    dit(A0, A1, logl, tw);
+    carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
+    for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
+    __syncthreads();
+    // W = m * N mod (R - 1): cyclic product of length H
+    dif(A0, A1, logl - 1, tw);
+    for (int i = tid; i < H; i += T) {
+        const int q = pad(i);
+        A0[q] = mont(A0[q], __ldg(cd.nh + i), P1, cc.pinv[0]);
+        A1[q] = mont(A1[q], __ldg(cd.nh + H + i), P2, cc.pinv[1]);
+    }
+    __syncthreads();
+    dit(A0, A1, logl - 1, tw);
+    const unsigned long long cW =
+        carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl - 1, cc); }, A0, cs);
+    // U = S1 + W (mod R - 1); S1 = X (square = false: S1 = x itself)
+    unsigned long long c = carry_pass<false>(
+        H, cS + cW, [&](int i) { return (unsigned long long)X[i] + A0[pad(i)]; }, X, cs);
+    while (c) {  // end-around carry: B^H == 1 (mod R - 1); at most two rounds
+        c = carry_pass<false>(H, c, [&](int i) { return (unsigned long long)X[i]; }, X, cs);
+    }
+    if (a > 1u) {
+        carry_pass<false>(H, 0ull, [&](int i) { return (unsigned long long)X[i] * a; }, X, cs);
+    }
+}
+
+}  // namespace mr
+}  // namespace pfb

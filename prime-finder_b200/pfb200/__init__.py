@@ -203,3 +203,101 @@ def unpack_mask(mask: np.ndarray, K: int) -> np.ndarray:
     """Packed mask block -> bool array [K, K] (True = eliminated)."""
     bits = np.unpackbits(np.asarray(mask, dtype=np.uint8)[: (K * K + 7) // 8], bitorder="little")
     return bits[: K * K].reshape(K, K).astype(bool)
+
+
+# ------------------------------------------------------------ Miller-Rabin ---
+
+MR_MAX_BITS = 22 * 8192 - 36
+
+
+class _Number(C.Structure):
+    """pfb_mr_number_t: { const uint16_t *limbs; int n_limbs; }"""
+    _fields_ = [("limbs", C.POINTER(C.c_uint16)), ("n_limbs", C.c_int)]
+
+
+def int_to_limbs16(x: int) -> np.ndarray:
+    n = max(1, (x.bit_length() + 15) // 16)
+    return np.frombuffer(x.to_bytes(2 * n, "little"), dtype="<u2").copy()
+
+
+def limbs16_to_int(a: np.ndarray) -> int:
+    return int.from_bytes(np.ascontiguousarray(a, dtype="<u2").tobytes(), "little")
+
+
+def _numbers(xs):
+    arrs = [x if isinstance(x, np.ndarray) else int_to_limbs16(int(x)) for x in xs]
+    arrs = [np.ascontiguousarray(a, dtype=np.uint16) for a in arrs]
+    st = (_Number * len(arrs))()
+    for i, a in enumerate(arrs):
+        st[i].limbs = a.ctypes.data_as(C.POINTER(C.c_uint16))
+        st[i].n_limbs = len(a)
+    return st, arrs
+
+
+def _mr_lib():
+    L = lib()
+    if not hasattr(L, "_mr_ready"):
+        vp = C.c_void_p
+        L.pfb_mr_create.argtypes = [C.POINTER(vp), C.c_int]
+        L.pfb_mr_create.restype = C.c_int
+        L.pfb_mr_destroy.argtypes = [vp]
+        L.pfb_mr_destroy.restype = None
+        L.pfb_mr_test.argtypes = [vp, C.POINTER(_Number), C.c_int, C.c_uint32,
+                                  C.POINTER(C.c_int8), C.POINTER(C.c_uint16), C.c_int]
+        L.pfb_mr_test.restype = C.c_int
+        L.pfb_mr_powm.argtypes = [vp, C.POINTER(_Number), C.c_int, C.c_uint32,
+                                  C.POINTER(_Number), C.POINTER(C.c_uint16), C.c_int]
+        L.pfb_mr_powm.restype = C.c_int
+        L.pfb_mr_test_cost.argtypes = [C.POINTER(C.c_uint16), C.c_int]
+        L.pfb_mr_test_cost.restype = C.c_longlong
+        L._mr_ready = True
+    return L
+
+
+class MillerRabin:
+    """Batched strong probable-prime tests on one GPU (pfb_mr_* C ABI)."""
+
+    def __init__(self, device: int = 0):
+        L = _mr_lib()
+        h = C.c_void_p()
+        _check(L.pfb_mr_create(C.byref(h), device), "pfb_mr_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _mr_lib().pfb_mr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def test(self, numbers, base: int = 2, residues: bool = True):
+        """Returns (verdicts, residues): verdict 1 = probable prime, 0 =
+        composite, -1 = invalid input; residue = base^d mod N (N-1 = 2^s d)."""
+        st, keep = _numbers(numbers)
+        n = len(keep)
+        ver = np.zeros(n, dtype=np.int8)
+        stride = max(len(a) for a in keep)
+        res = np.zeros(n * stride, dtype=np.uint16) if residues else None
+        rc = _mr_lib().pfb_mr_test(self._h, st, n, base, ver.ctypes.data_as(C.POINTER(C.c_int8)),
+                                   res.ctypes.data_as(C.POINTER(C.c_uint16)) if residues else None,
+                                   stride)
+        _check(rc, "pfb_mr_test")
+        out = None
+        if residues:
+            out = [limbs16_to_int(res[i * stride:(i + 1) * stride]) for i in range(n)]
+        return ver.tolist(), out
+
+    def powm(self, numbers, exps, base: int = 2):
+        st, keep = _numbers(numbers)
+        se, keep_e = _numbers(exps)
+        n = len(keep)
+        stride = max(len(a) for a in keep)
+        res = np.zeros(n * stride, dtype=np.uint16)
+        rc = _mr_lib().pfb_mr_powm(self._h, st, n, base, se,
+                                   res.ctypes.data_as(C.POINTER(C.c_uint16)), stride)
+        _check(rc, "pfb_mr_powm")
+        return [limbs16_to_int(res[i * stride:(i + 1) * stride]) for i in range(n)]

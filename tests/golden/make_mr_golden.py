@@ -1,0 +1,71 @@
+"""Regenerate the full-size Miller-Rabin golden fixtures with GMP.
+
+For every number listed below this computes, with GMP 6.3 mpz_powm (through
+oracle/mr_oracle.c), the base-2 strong-test residue r = 2^d mod N
+(N - 1 = 2^s d) and the verdicts, and stores a SHA-256 of r (little-endian
+16-bit limbs, ceil(bits(N)/16) of them) plus its low 64 bits:
+
+  mr_config1.json  N and rev(N) of the first 16 (k,j) survivors of the
+                   (50000, 30000, 100) sieve (the reference's own
+                   miller_rabin_test verdicts are stored beside them)
+  mr_config3.json  N and rev(N) of every survivor (k,j <= 99) of that sieve:
+                   the candidates the 256-number uniform batch draws from
+
+Each 50 000-digit powm takes minutes of one core; the script runs a process
+pool (spawn) over all cores.  Usage:
+  python tests/golden/make_mr_golden.py config1|config3
+"""
+import hashlib
+import json
+import multiprocessing as mp
+import os
+import sys
+import time
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+
+def residue_record(args):
+    import oracle
+    a, b, c, k, j, rev = args
+    N = oracle.build_candidate(a, b, c, k, j, rev)
+    t0 = time.time()
+    s, r = oracle.strong_residue(N, 2)
+    n16 = (N.bit_length() + 15) // 16
+    rb = r.to_bytes(2 * n16, "little")
+    verdict = 1 if (r == 1 or r == N - 1) else 0
+    if not verdict and s > 1:
+        verdict = oracle.strong_test(N, 2)
+    return {"a": a, "b": b, "c": c, "k": k, "j": j, "rev": int(rev), "bits": N.bit_length(),
+            "s": s, "sha256": hashlib.sha256(rb).hexdigest(), "low64": "%016x" % (r & (2**64 - 1)),
+            "sprp2": verdict, "secs": round(time.time() - t0, 1)}
+
+
+def main():
+    which = sys.argv[1] if len(sys.argv) > 1 else "config1"
+    sv = json.load(open(os.path.join(HERE, "sieve_config1.json")))
+    a, b, c = sv["abc"]
+    pairs = [tuple(x) for x in sv["survivors_99"]]
+    if which == "config1":
+        pairs = pairs[:16]
+    jobs = [(a, b, c, k, j, rev) for (k, j) in pairs for rev in (False, True)]
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(os.cpu_count()) as pool:
+        recs = pool.map(residue_record, jobs, chunksize=1)
+    out = {"source": "GMP 6.3 mpz_powm via oracle/mr_oracle.c", "base": 2, "abc": [a, b, c],
+           "records": recs}
+    if which == "config1":
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle
+        if oracle.ref_available():
+            out["ref_miller_rabin_test"] = {"%d,%d" % p: oracle.ref_miller_rabin_test(a, b, c, *p)
+                                            for p in pairs}
+    with open(os.path.join(HERE, "mr_%s.json" % which), "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", len(recs), "records")
+
+
+if __name__ == "__main__":
+    main()

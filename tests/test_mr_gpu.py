@@ -1,0 +1,172 @@
+"""GPU parity of the Miller-Rabin engine against GMP (the oracle).
+
+Mirrors miller_rabin_gpu/correctness_tests.cuh: modular powers against
+mpz_powm (:578-639 uses x^0xDEADBEEF), Mersenne primes M521/M607/M1279
+through all 16 default witnesses (:762-834), primes with s = 1 and s > 1
+generated by mpz_nextprime above 2^512 (:842-1031), plus random composites.
+Residues are compared word for word; verdicts bit for bit.
+"""
+import hashlib
+import json
+import os
+import random
+
+import numpy as np
+import pytest
+
+import oracle
+import pfb200
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+WITNESSES = [2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37, 41, 43, 47, 53]  # runner.cuh:15-16
+
+
+@pytest.fixture(scope="module")
+def mr():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    e = pfb200.MillerRabin(0)
+    yield e
+    e.close()
+
+
+def _gmp_powm(base, E, N):
+    bl = oracle.int_to_limbs(base, 1)
+    el = oracle.int_to_limbs(E, (E.bit_length() + 15) // 16)
+    n16 = (N.bit_length() + 15) // 16
+    nl = oracle.int_to_limbs(N, n16)
+    out = np.zeros(n16, dtype=np.uint16)
+    L = oracle.lib()
+    L.oracle_powm(oracle._ptr(bl, oracle.C.c_uint16), 1, oracle._ptr(el, oracle.C.c_uint16), len(el),
+                  oracle._ptr(nl, oracle.C.c_uint16), n16, oracle._ptr(out, oracle.C.c_uint16))
+    return oracle.limbs_to_int(out)
+
+
+def test_powm_small_vs_gmp(mr):
+    rng = random.Random(0xDEADBEEF)
+    Ns, Es = [], []
+    for bits in (3, 17, 64, 100, 521, 1000, 2000, 2790, 2800, 3000, 5000, 9000):
+        N = rng.getrandbits(bits) | (1 << (bits - 1)) | 1
+        Ns.append(N)
+        Es.append(rng.getrandbits(rng.randint(1, 300)) | 1)
+    Es[0] = 0xDEADBEEF
+    for base in (2, 3, 53, 65535):
+        got = mr.powm(Ns, Es, base)
+        for N, E, r in zip(Ns, Es, got):
+            assert r == pow(base, E, N) == _gmp_powm(base, E, N), (base, N.bit_length())
+
+
+def test_powm_long_exponent(mr):
+    rng = random.Random(7)
+    N = rng.getrandbits(4000) | (1 << 3999) | 1
+    E = rng.getrandbits(4000)
+    assert mr.powm([N], [E], 2)[0] == pow(2, E, N)
+
+
+def test_residue_equals_gmp_strong_residue(mr):
+    rng = random.Random(11)
+    Ns = [rng.getrandbits(b) | (1 << (b - 1)) | 1 for b in (200, 700, 1500, 2790, 2900, 6000)]
+    for base in (2, 3):
+        ver, res = mr.test(Ns, base)
+        for N, v, r in zip(Ns, ver, res):
+            s, rg = oracle.strong_residue(N, base)
+            assert r == rg
+            assert v == oracle.strong_test(N, base)
+
+
+def test_mersenne_primes_all_witnesses(mr):
+    Ms = [(1 << p) - 1 for p in (521, 607, 1279)]
+    for a in WITNESSES:
+        ver, _ = mr.test(Ms, a, residues=False)
+        assert ver == [1, 1, 1], a
+
+
+def test_nextprime_kats_s1_and_general_s(mr):
+    base = 1 << 512
+    primes = []
+    p = base + 3
+    while len(primes) < 3:  # s = 1 primes (p == 3 mod 4), correctness_tests.cuh:959-1031
+        p = oracle.nextprime(p)
+        if (p - 1) % 4 == 2:
+            primes.append(p)
+    for target in (2, 3, 4):  # s = 2, 3, >= 4
+        p = base + 1
+        while True:
+            p = oracle.nextprime(p)
+            s = ((p - 1) & -(p - 1)).bit_length() - 1
+            if (target < 4 and s == target) or (target == 4 and s >= 4):
+                primes.append(p)
+                break
+    for a in WITNESSES[:6]:
+        ver, res = mr.test(primes, a)
+        assert ver == [1] * len(primes), a
+        for N, r in zip(primes, res):
+            assert r == oracle.strong_residue(N, a)[1]
+
+
+def test_random_composites_and_strong_pseudoprimes(mr):
+    rng = random.Random(5)
+    Ns = [rng.getrandbits(900) | (1 << 899) | 1 for _ in range(20)]
+    Ns += [2047, 3277, 4033, 4681, 8321]  # base-2 strong pseudoprimes
+    Ns += [3215031751, 25326001]           # pseudoprimes to several small bases
+    for a in (2, 3, 5):
+        ver, _ = mr.test(Ns, a, residues=False)
+        assert ver == [oracle.strong_test(N, a) for N in Ns], a
+
+
+def test_mixed_lengths_one_batch(mr):
+    rng = random.Random(9)
+    Ns = []
+    for bits in (40, 2700, 2760, 5800, 11000, 23000, 45000, 90000, 150000, 166096):
+        Ns.append(rng.getrandbits(bits) | (1 << (bits - 1)) | 1)
+    Es = [rng.getrandbits(64) | 1 for _ in Ns]
+    got = mr.powm(Ns, Es, 2)
+    for N, E, r in zip(Ns, Es, got):
+        assert r == pow(2, E, N), N.bit_length()
+
+
+def test_invalid_inputs_flagged(mr):
+    ver, _ = mr.test([10, 1, 7, 1 << 200, (1 << pfb200.MR_MAX_BITS + 1) + 1], 2, residues=False)
+    assert ver == [-1, -1, 1, -1, -1]
+
+
+def test_bucket_boundaries(mr):
+    # largest modulus of each transform length, and one bit more
+    rng = random.Random(13)
+    Ns = []
+    for lg in range(8, 15):
+        rb = 22 * (1 << (lg - 1))
+        for bits in (rb - 36, rb - 35):
+            Ns.append(rng.getrandbits(bits) | (1 << (bits - 1)) | 1)
+    Es = [0xDEADBEEF for _ in Ns]
+    got = mr.powm(Ns, Es, 2)
+    for N, r in zip(Ns, got):
+        assert r == pow(2, 0xDEADBEEF, N)
+
+
+def _golden(name):
+    path = os.path.join(GOLD, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} not generated")
+    return json.load(open(path))
+
+
+def test_config1_full_size_residues(mr):
+    """50 000-digit N and rev(N) of the first 16 sieve survivors: residues
+    2^d mod N must hash to the GMP values and verdicts match the reference."""
+    g = _golden("mr_config1.json")
+    recs = g["records"]
+    Ns = [oracle.build_candidate(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs]
+    ver, res = mr.test(Ns, 2)
+    for r, N, v, x in zip(recs, Ns, ver, res):
+        n16 = (N.bit_length() + 15) // 16
+        assert hashlib.sha256(x.to_bytes(2 * n16, "little")).hexdigest() == r["sha256"], (r["k"], r["j"])
+        assert v == r["sprp2"]
+    if "ref_miller_rabin_test" in g:
+        for i in range(0, len(recs), 2):
+            k, j = recs[i]["k"], recs[i]["j"]
+            want = g["ref_miller_rabin_test"]["%d,%d" % (k, j)]
+            got = 0 if ver[i] == 0 else (2 if ver[i + 1] == 1 else 1)
+            assert got == want
