@@ -93,13 +93,20 @@ __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, Twiddles
 }
 
 // Canonical residue of X (Montgomery form) into Y: Y = X R^-1 mod N.
-__device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const Twiddles &tw) {
+__device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uint32_t *nl, const Twiddles &tw) {
     const int H = 1 << (cd.logl - 1);
     for (int i = threadIdx.x; i < H; i += blockDim.x) Y[i] = sm.X[i];
     __syncthreads();
     Smem s2 = sm;
     s2.X = Y;
     mont_step(s2, cd, false, 1u, tw, c_crt);
+    // REDC(X) lies in [0, N]; it is N only when X == 0 (mod N), e.g. a base
+    // that is a multiple of N.  Map it to 0.
+    bool eqn = true;
+    for (int i = threadIdx.x; i < H; i += blockDim.x) eqn = eqn && (Y[i] == nl[i]);
+    if (__syncthreads_and(eqn))
+        for (int i = threadIdx.x; i < H; i += blockDim.x) Y[i] = 0u;
+    __syncthreads();
 }
 
 __global__ void __launch_bounds__(THREADS, 1) step_kernel(JobDev *jobs, int max_steps, Twiddles tw) {
@@ -127,7 +134,7 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel(JobDev *jobs, int max_
                 mont_step(sm, cd, true, 1u, tw, c_crt);
                 extra--;
             }
-            canonical(sm, Y, cd, tw);
+            canonical(sm, Y, cd, jb.nl, tw);
             // compare with 1 and N - 1 (N odd: N - 1 differs from N in limb 0 only)
             bool one = true, nm1 = true;
             for (int i = threadIdx.x; i < H; i += blockDim.x) {
@@ -203,7 +210,7 @@ static void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const
     if (!num.limbs || num.n_limbs <= 0) return;
     Words N = from_u16(num.limbs, (size_t)num.n_limbs);
     const size_t nb = bit_length(N);
-    if (nb < 2 || !(N[0] & 1ull)) return;
+    if (nb < 2 || !(N[0] & 1ull) || nb > (size_t)PFB_MR_MAX_BITS) return;
     const int lg = choose_logl(nb, base);
     if (lg < 0) return;
     const size_t H = (size_t)1 << (lg - 1);

@@ -194,7 +194,7 @@ template <bool PAD, class Get>
 __device__ unsigned long long carry_pass(const int n, const unsigned long long cin0, Get get, uint32_t *out,
                                          CarrySmem &cs) {
     const int T = blockDim.x;
-    const int w = n >= T ? n / T : 1;
+    const int w = n >= 2 * T ? n / T : 2;  // >= 2 limbs: a carry-in (< 2^41) never overflows a segment twice
     const int na = n / w;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const unsigned FULL = 0xffffffffu;
@@ -212,8 +212,7 @@ __device__ unsigned long long carry_pass(const int n, const unsigned long long c
             else if (q == 1) l1 = limb;
             else ones = ones && (limb == LIMB_MASK);
         }
-        if (w == 1) room = (1ull << LIMB_BITS) - l0;
-        else if (ones) room = (1ull << (2 * LIMB_BITS)) - ((unsigned long long)l1 << LIMB_BITS) - l0;
+        if (ones) room = (1ull << (2 * LIMB_BITS)) - ((unsigned long long)l1 << LIMB_BITS) - l0;
     }
     unsigned long long prev = __shfl_up_sync(FULL, acc, 1);
     if (lane == 31) cs.wc[warp] = acc;
