@@ -61,80 +61,144 @@ __device__ __forceinline__ uint32_t mont(uint32_t a, uint32_t b, uint32_t p, uin
 
 __device__ __forceinline__ uint32_t red2(uint32_t x, uint32_t p2) { return x >= p2 ? x - p2 : x; }
 
-// Radix-2^RLOG decimation-in-frequency pass over both primes (natural order in,
-// bit-reversed out after all passes).  h0 = half size of the first stage.
-template <int RLOG>
-__device__ __forceinline__ void dif_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
+// Twiddles of one radix-2^RLOG group: stage s uses omega_{2 hs}^j for
+// j = j0 + e * sub (DIF) or j0 + e * h0 (DIT), e < 2^s or 2^(RLOG-1-s).
+template <int RLOG, bool DIT>
+__device__ __forceinline__ void load_tw(const uint32_t *__restrict__ W, const uint32_t *__restrict__ Wsh, int j0,
+                                        int step, int lh0, uint32_t *tw, uint32_t *tws) {
+    constexpr int R = 1 << RLOG;
+#pragma unroll
+    for (int s = 0, t = 0; s < RLOG; s++) {
+        const int cnt = DIT ? (1 << s) : (R >> (s + 1));
+        const int shift = DIT ? LOG_LMAX - 1 - (lh0 + s) : LOG_LMAX - 1 - (lh0 - s);
+#pragma unroll
+        for (int e = 0; e < cnt; e++, t++) {
+            const int k = (j0 + e * step) << shift;
+            tw[t] = __ldg(W + k);
+            tws[t] = __ldg(Wsh + k);
+        }
+    }
+}
+
+template <int PR, int RLOG>
+__device__ __forceinline__ void dif_group(uint32_t *__restrict__ A, int base, int sub, const uint32_t *tw,
+                                          const uint32_t *tws) {
+    constexpr int R = 1 << RLOG;
+    constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
+    uint32_t v[R];
+#pragma unroll
+    for (int e = 0; e < R; e++) v[e] = A[pad(base + e * sub)];
+#pragma unroll
+    for (int s = 0, t0 = 0; s < RLOG; t0 += R >> (s + 1), s++) {
+        const int half = R >> (s + 1);
+#pragma unroll
+        for (int e = 0; e < R; e++) {
+            if (e & half) continue;
+            const int t = t0 + (e & (half - 1));
+            const uint32_t x = v[e], y = v[e + half];
+            v[e] = red2(x + y, p2);
+            v[e + half] = shoup(x - y + p2, tw[t], tws[t], p);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < R; e++) A[pad(base + e * sub)] = v[e];
+}
+
+template <int PR, int RLOG>
+__device__ __forceinline__ void dit_group(uint32_t *__restrict__ A, int base, int h0, const uint32_t *tw,
+                                          const uint32_t *tws) {
+    constexpr int R = 1 << RLOG;
+    constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
+    uint32_t v[R];
+#pragma unroll
+    for (int e = 0; e < R; e++) v[e] = A[pad(base + e * h0)];
+#pragma unroll
+    for (int s = 0, t0 = 0; s < RLOG; t0 += 1 << s, s++) {
+        const int half = 1 << s;
+#pragma unroll
+        for (int e = 0; e < R; e++) {
+            if (e & half) continue;
+            const int t = t0 + (e & (half - 1));
+            const uint32_t x = v[e];
+            const uint32_t u = shoup(v[e + half], tw[t], tws[t], p);
+            v[e] = red2(x + u, p2);
+            v[e + half] = red2(x - u + p2, p2);
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < R; e++) A[pad(base + e * h0)] = v[e];
+}
+
+// Radix-2^RLOG decimation-in-frequency pass for prime PR over groups
+// g0, g0 + stride, ... (natural order in, bit-reversed out after all passes).
+// h0 = half size of the first stage.  When every group of this thread has the
+// same j0 (all passes but the widest) the twiddles are loaded once per pass.
+template <int PR, int RLOG>
+__device__ __forceinline__ void dif_pass1(uint32_t *__restrict__ A, int logn, int h0,
+                                          const uint32_t *__restrict__ W, const uint32_t *__restrict__ Wsh,
+                                          int g0, int stride) {
     constexpr int R = 1 << RLOG;
     const int groups = (1 << logn) >> RLOG;
     const int sub = (2 * h0) >> RLOG;  // element stride inside a group
     const int lh0 = 31 - __clz(h0);
-    for (int g = threadIdx.x; g < 2 * groups; g += blockDim.x) {
-        const int pr = g >= groups;
-        const int gg = g - (pr ? groups : 0);
-        uint32_t *A = pr ? A1 : A0;
-        const uint32_t p = pr ? P2 : P1, p2 = 2u * p;
-        const uint32_t *W = tw.w[pr], *Wsh = tw.wsh[pr];
-        const int block = gg / sub, j0 = gg - block * sub;
-        const int base = block * 2 * h0 + j0;
-        uint32_t v[R];
-#pragma unroll
-        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * sub)];
-#pragma unroll
-        for (int s = 0; s < RLOG; s++) {
-            const int half = R >> (s + 1);
-            const int shift = LOG_LMAX - 1 - (lh0 - s);  // k = j << shift
-#pragma unroll
-            for (int e = 0; e < R; e++) {
-                if (e & half) continue;
-                const int j = j0 + (e & (half - 1)) * sub;
-                const int k = j << shift;
-                const uint32_t x = v[e], y = v[e + half];
-                v[e] = red2(x + y, p2);
-                v[e + half] = shoup(x - y + p2, __ldg(W + k), __ldg(Wsh + k), p);
-            }
+    uint32_t ta[R - 1], tsa[R - 1];
+    if (stride % sub == 0) {
+        load_tw<RLOG, false>(W, Wsh, g0 % sub, sub, lh0, ta, tsa);
+        for (int gg = g0; gg < groups; gg += stride) {
+            const int block = gg / sub, j0 = gg - block * sub;
+            dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
         }
-#pragma unroll
-        for (int e = 0; e < R; e++) A[pad(base + e * sub)] = v[e];
+        return;
+    }
+    for (int gg = g0; gg < groups; gg += stride) {
+        const int block = gg / sub, j0 = gg - block * sub;
+        load_tw<RLOG, false>(W, Wsh, j0, sub, lh0, ta, tsa);
+        dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
     }
 }
 
-// Radix-2^RLOG decimation-in-time pass (bit-reversed in, natural out); h0 =
-// half size of the first (smallest) stage.
-template <int RLOG>
-__device__ __forceinline__ void dit_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
+// Radix-2^RLOG decimation-in-time pass for prime PR (bit-reversed in, natural
+// out); h0 = half size of the first (smallest) stage.
+template <int PR, int RLOG>
+__device__ __forceinline__ void dit_pass1(uint32_t *__restrict__ A, int logn, int h0,
+                                          const uint32_t *__restrict__ W, const uint32_t *__restrict__ Wsh,
+                                          int g0, int stride) {
     constexpr int R = 1 << RLOG;
     const int groups = (1 << logn) >> RLOG;
     const int lh0 = 31 - __clz(h0);
-    for (int g = threadIdx.x; g < 2 * groups; g += blockDim.x) {
-        const int pr = g >= groups;
-        const int gg = g - (pr ? groups : 0);
-        uint32_t *A = pr ? A1 : A0;
-        const uint32_t p = pr ? P2 : P1, p2 = 2u * p;
-        const uint32_t *W = tw.wi[pr], *Wsh = tw.wish[pr];
-        const int block = gg >> lh0, j0 = gg & (h0 - 1);
-        const int base = block * R * h0 + j0;
-        uint32_t v[R];
-#pragma unroll
-        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * h0)];
-#pragma unroll
-        for (int s = 0; s < RLOG; s++) {
-            const int half = 1 << s;
-            const int shift = LOG_LMAX - 1 - (lh0 + s);
-#pragma unroll
-            for (int e = 0; e < R; e++) {
-                if (e & half) continue;
-                const int j = j0 + (e & (half - 1)) * h0;
-                const int k = j << shift;
-                const uint32_t x = v[e];
-                const uint32_t t = shoup(v[e + half], __ldg(W + k), __ldg(Wsh + k), p);
-                v[e] = red2(x + t, p2);
-                v[e + half] = red2(x - t + p2, p2);
-            }
+    uint32_t ta[R - 1], tsa[R - 1];
+    if (stride % h0 == 0) {
+        load_tw<RLOG, true>(W, Wsh, g0 & (h0 - 1), h0, lh0, ta, tsa);
+        for (int gg = g0; gg < groups; gg += stride) {
+            const int block = gg >> lh0, j0 = gg & (h0 - 1);
+            dit_group<PR, RLOG>(A, block * R * h0 + j0, h0, ta, tsa);
         }
-#pragma unroll
-        for (int e = 0; e < R; e++) A[pad(base + e * h0)] = v[e];
+        return;
     }
+    for (int gg = g0; gg < groups; gg += stride) {
+        const int j0 = gg & (h0 - 1);
+        load_tw<RLOG, true>(W, Wsh, j0, h0, lh0, ta, tsa);
+        dit_group<PR, RLOG>(A, (gg >> lh0) * R * h0 + j0, h0, ta, tsa);
+    }
+}
+
+// Both primes in one pass: threads [0, T/2) work on A0 (p1), [T/2, T) on A1 (p2).
+template <int RLOG>
+__device__ __forceinline__ void dif_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
+    const int half = blockDim.x >> 1;
+    if ((int)threadIdx.x < half)
+        dif_pass1<0, RLOG>(A0, logn, h0, tw.w[0], tw.wsh[0], threadIdx.x, half);
+    else
+        dif_pass1<1, RLOG>(A1, logn, h0, tw.w[1], tw.wsh[1], threadIdx.x - half, half);
+}
+
+template <int RLOG>
+__device__ __forceinline__ void dit_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
+    const int half = blockDim.x >> 1;
+    if ((int)threadIdx.x < half)
+        dit_pass1<0, RLOG>(A0, logn, h0, tw.wi[0], tw.wish[0], threadIdx.x, half);
+    else
+        dit_pass1<1, RLOG>(A1, logn, h0, tw.wi[1], tw.wish[1], threadIdx.x - half, half);
 }
 
 __device__ void dif(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
@@ -203,14 +267,20 @@ __device__ unsigned long long carry_pass(const int n, const unsigned long long c
         const int lo = t * w;
         uint32_t l0 = 0, l1 = 0;
         bool ones = true;
-        for (int q = 0; q < w; q++) {
-            acc += get(lo + q);
-            const uint32_t limb = (uint32_t)acc & LIMB_MASK;
-            acc >>= LIMB_BITS;
-            out[PAD ? pad(lo + q) : lo + q] = limb;
-            if (q == 0) l0 = limb;
-            else if (q == 1) l1 = limb;
-            else ones = ones && (limb == LIMB_MASK);
+        for (int q = 0; q < w; q += 2) {  // w is even
+            unsigned long long vv[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) vv[u] = get(lo + q + u);
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                acc += vv[u];
+                const uint32_t limb = (uint32_t)acc & LIMB_MASK;
+                acc >>= LIMB_BITS;
+                out[PAD ? pad(lo + q + u) : lo + q + u] = limb;
+                if (q + u == 0) l0 = limb;
+                else if (q + u == 1) l1 = limb;
+                else ones = ones && (limb == LIMB_MASK);
+            }
         }
         if (ones) room = (1ull << (2 * LIMB_BITS)) - ((unsigned long long)l1 << LIMB_BITS) - l0;
     }
