@@ -1,0 +1,440 @@
+#!/usr/bin/env python
+"""Benchmark of the two hot paths on B200.
+
+Headline (value): base-2 strong probable-prime tests per second of the
+served, batched Miller-Rabin engine on the uniform 50 000-digit batch: 256
+candidates, N and rev(N) for 128 (k,j) drawn with splitmix64(seed=1) from the
+sieve survivors (k,j <= 99) of (a,b,c) = (50000, 30000, 100).  The survivors
+come from this repository's own GPU sieve over every odd prime below 1e8.
+
+A step is `--chunk` modular squarings of every candidate of the resident
+batch; tests/s = candidates * squarings done / squarings per test / time.
+Beside it the line reports:
+  e2e          complete tests through the C ABI (pfb_mr_test) from host limbs:
+               host set-up, H2D, every squaring, verdict + residue D2H
+  plain        the one-candidate-per-call form on the same GPU
+  sieve        K = 9999 grid pairs/s over the (a,b,c) triples of the
+               config-2 enumeration, and the drop-in 100 x 100 call
+  roofline     INT32 multiplies of the reference's squaring structure
+               (6 length-L transforms + 3 pointwise products, 2 primes, 3
+               multiplies per modmul, L = 32768 at 50 000 digits) per second,
+               over this device's measured INT32 multiply peak
+  cpu_baseline GMP 6.3 mpz_powm on the host cores, sampled
+
+Multi-GPU: one process per GPU (torchrun), each an independent replica
+(weak scaling); the time is the max over ranks.
+"""
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "prime-finder_b200"))
+
+SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference count)
+
+
+def splitmix64(seed):
+    x = seed & (2**64 - 1)
+    while True:
+        x = (x + 0x9E3779B97F4A7C15) & (2**64 - 1)
+        z = x
+        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
+        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
+        yield z ^ (z >> 31)
+
+
+def ref_modmuls_per_squaring(digits: int) -> int:
+    """Modmuls of one squaring in the reference's structure (16-bit limbs,
+    limbs_for_digits + padding to a power of two, 6 transforms, 3 pointwise
+    products, 2 word primes): M(L) = 2 (6 (L/2) log2 L + 3 L)."""
+    limbs = int((digits * 3.32193 + 15) / 16) + 4
+    L = 1
+    while L < 2 * limbs:
+        L *= 2
+    lg = L.bit_length() - 1
+    return 2 * (6 * (L // 2) * lg + 3 * L)
+
+
+# --------------------------------------------------------------- clocks ----
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------- CPU baseline ---
+
+def _gmp_powm_sample(args):
+    a, b, c, k, j, rev, sample_bits = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import oracle
+    N = oracle.build_candidate(a, b, c, k, j, rev)
+    d = (N - 1) >> 1
+    E = d >> max(0, d.bit_length() - sample_bits)
+    n16 = (N.bit_length() + 15) // 16
+    nl = oracle.int_to_limbs(N, n16)
+    el = oracle.int_to_limbs(E, (E.bit_length() + 15) // 16)
+    bl = oracle.int_to_limbs(2, 1)
+    out = np.zeros(n16, dtype=np.uint16)
+    L = oracle.lib()
+    t0 = time.perf_counter()
+    L.oracle_powm(oracle._ptr(bl, oracle.C.c_uint16), 1, oracle._ptr(el, oracle.C.c_uint16), len(el),
+                  oracle._ptr(nl, oracle.C.c_uint16), n16, oracle._ptr(out, oracle.C.c_uint16))
+    dt = time.perf_counter() - t0
+    return dt / E.bit_length(), d.bit_length()
+
+
+def cpu_mr_baseline(pairs, abc, sample_bits=4096, procs=None):
+    """GMP mpz_powm(2, d, N) on every host core at once, each on the top
+    `sample_bits` bits of d; scaled to full tests (bits(d) squarings)."""
+    procs = procs or os.cpu_count() or 1
+    jobs = [(abc[0], abc[1], abc[2], pairs[i % len(pairs)][0], pairs[i % len(pairs)][1], bool(i & 1),
+             sample_bits) for i in range(procs)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_gmp_powm_sample, jobs)
+    wall = time.perf_counter() - t0
+    per_core = [1.0 / (t_sq * bits) for t_sq, bits in res]
+    return {"value": sum(per_core), "unit": "tests/s", "cores": procs, "kind": "port",
+            "per_core": statistics.mean(per_core),
+            "sample": "GMP 6.3 mpz_powm(2, top %d bits of d, N) for N, rev(N) of the 50 000-digit "
+                      "batch, one process per core, scaled to bits(d) squarings per test (%.1f s wall)"
+                      % (sample_bits, wall)}
+
+
+def _sieve_ref_sample(args):
+    frac_primes, a, b, c = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    P = oracle.primes_below(100_000_000)
+    sub = P[: int(len(P) * frac_primes)]
+    t0 = time.perf_counter()
+    oracle.ref_trial_div_cpu(sub, a, b, c)
+    return (time.perf_counter() - t0) / len(sub), len(P)
+
+
+def cpu_sieve_baseline(procs=None, frac=0.05):
+    """The reference's own trial_div_cpu (100 x 100 grid) on every core, each on
+    a 5% prefix of the primes, scaled to the whole list: pairs/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return None
+    procs = procs or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(procs) as pool:
+        res = pool.map(_sieve_ref_sample, [(frac, 50000 + i, 30000, 100) for i in range(procs)])
+    per_core = [1e4 / (t_p * n) for t_p, n in res]
+    return {"value": sum(per_core), "unit": "pairs/s", "cores": procs, "kind": "reference",
+            "sample": "reference trial_div_cpu (100x100 grid) on the first %d%% of the primes < 1e8, "
+                      "one process per core, scaled by prime count" % int(frac * 100)}
+
+
+# ------------------------------------------------------------ workloads ----
+
+def config3_pairs(survivors):
+    g = splitmix64(1)
+    return [survivors[next(g) % len(survivors)] for _ in range(128)]
+
+
+def config2_triples(n):
+    """(a,b,c) of the config-2 enumeration: a in [50000, 50063]; per a, c = 100,
+    b = c+1, c+1+997, ...; the first n triples taken a-major over b."""
+    out = []
+    i = 0
+    while len(out) < n:
+        a = 50000 + (i % 64)
+        bi = i // 64
+        c = 100
+        b = c + 1 + 997 * bi
+        if b <= a - 1:
+            out.append((a, b, c))
+        i += 1
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--chunk", type=int, default=1024, help="squarings per candidate per step")
+    ap.add_argument("--e2e-batch", type=int, default=0, help="candidates in the e2e call (0 = one per SM)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--sieve-triples", type=int, default=4)
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    abc1 = (50000, 30000, 100)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        import json as _j
+        g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_config1.json")))
+        pairs = [tuple(x) for x in g["survivors_99"]]
+        t0 = time.perf_counter()
+        steps = []
+        for _ in range(args.warmup + args.steps):
+            steps.append(cpu_mr_baseline(config3_pairs(pairs), abc1, sample_bits=1024))
+        vals = [s["value"] for s in steps[args.warmup:]]
+        v = statistics.mean(vals)
+        last = steps[-1]
+        print(json.dumps({
+            "impl": "reference", "metric": "MR base-2 tests/s, 50 000-digit batch (config 3)",
+            "value": v, "unit": "tests/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * (time.perf_counter() - t0) / max(1, len(steps)), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {"workload": "uniform MR batch: 256 x 50 000-digit N/rev(N) of (50000,30000,100) survivors"},
+            "cpu_baseline": {"kind": last["kind"], "cores": last["cores"], "sample": last["sample"], "value": v,
+                             "unit": "tests/s"},
+            "e2e": {"value": v, "unit": "tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    # CPU baselines first: spawn pools before CUDA is initialised in this process
+    cpu = None
+    cpu_sieve = None
+    if rank == 0 and not args.no_cpu:
+        import json as _j
+        g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_config1.json")))
+        pairs = [tuple(x) for x in g["survivors_99"]]
+        cpu = cpu_mr_baseline(config3_pairs(pairs), abc1, sample_bits=4096)
+        cpu_sieve = cpu_sieve_baseline()
+
+    import numpy as np
+    import torch
+    import pfb200
+
+    torch.cuda.set_device(local)
+    dev = local
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    # primes for the sieve: generated by a plain Eratosthenes in numpy (input data)
+    lim = 100_000_000
+    sieve = np.ones(lim // 2 + 1, dtype=bool)
+    sieve[0] = False
+    for i in range(1, int(lim ** 0.5) // 2 + 1):
+        if sieve[i]:
+            p = 2 * i + 1
+            sieve[p * p // 2::p] = False
+    primes = (2 * np.nonzero(sieve)[0] + 1).astype(np.uint32)
+    primes = primes[primes <= lim]
+
+    # --- sieve -------------------------------------------------------------
+    sv = pfb200.Sieve(primes, dev)
+    m100 = sv.run([abc1], 100)
+    ok = pfb200.unpack_mask(m100, 100)
+    survivors = [(k + 1, j + 1) for k in range(99) for j in range(99) if not ok[k, j]]
+    K = 9999
+    stream = torch.cuda.Stream()
+    blk = pfb200.mask_bytes(K)
+    ntr = args.sieve_triples
+    dmask = torch.zeros(blk * ntr, dtype=torch.uint8, device="cuda")
+    sieve_launches = 0
+    with torch.cuda.stream(stream):
+        triples = config2_triples(ntr * (args.steps + args.warmup))
+        for w in range(args.warmup):
+            sv.run(triples[w * ntr:(w + 1) * ntr], K, dmask, stream=stream.cuda_stream)
+        stream.synchronize()
+        times = []
+        for s in range(args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            tr = triples[(args.warmup + s) * ntr:(args.warmup + s + 1) * ntr]
+            e0.record(stream)
+            sv.run(tr, K, dmask, stream=stream.cuda_stream)
+            e1.record(stream)
+            stream.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    sieve_pairs_s = ntr * K * K * len(times) / max_over_ranks(sum(times)) * world
+    t = pfb200.GpuTiming()
+    pfb200.trial_div_gpu(primes, *abc1, None, t)
+    t0 = time.perf_counter()
+    for _ in range(3):
+        pfb200.trial_div_gpu(primes, *abc1, None, t)
+    dropin_s = (time.perf_counter() - t0) / 3
+
+    # --- Miller-Rabin: resident batch ---------------------------------------
+    pairs = config3_pairs(survivors)
+    cands = [pfb200.build_candidate(*abc1, k, j, rev) for (k, j) in pairs for rev in (False, True)]
+    sq_per_test = statistics.mean([(N - 1).bit_length() for N in cands])  # bits(d) + 1 check, s = 1
+    eng = pfb200.MillerRabin(dev)
+    batch = pfb200.MRBatch(eng, cands, 2)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
+    chunk = args.chunk
+    launches_per_step = (chunk + 2047) // 2048
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            batch.advance(chunk, stream.cuda_stream)
+        stream.synchronize()
+        barrier()
+        times = []
+        with ClockSampler(dev) as clocks:
+            for _ in range(args.steps):
+                flush.fill_(1)  # L2 flush between timed steps (outside the events)
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                batch.advance(chunk, stream.cuda_stream)
+                e1.record(stream)
+                stream.synchronize()
+                times.append(e0.elapsed_time(e1) / 1e3)
+        barrier()
+    t_mr = max_over_ranks(sum(times))
+    n = len(cands)
+    squarings = n * chunk * args.steps
+    tests_s = squarings / sq_per_test / t_mr * world
+    ms_per_step = 1e3 * t_mr / args.steps
+    batch.close()
+
+    # plain form: one candidate per call
+    one = pfb200.MRBatch(eng, cands[:1], 2)
+    with torch.cuda.stream(stream):
+        one.advance(256, stream.cuda_stream)
+        stream.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one.advance(1024, stream.cuda_stream)
+        e1.record(stream)
+        stream.synchronize()
+    plain_sq_s = 1024 / (e0.elapsed_time(e1) / 1e3)
+    plain_tests_s = plain_sq_s / sq_per_test
+    one.close()
+
+    # roofline of the squaring kernel
+    peak_lo, peak_hi = pfb200.measure_int32_peak(dev)
+    digits = len(str(cands[0]))
+    ref_mults = ref_modmuls_per_squaring(digits) * SQ_PER_MODMUL
+    achieved = squarings / t_mr * ref_mults  # INT32 multiplies / s (one GPU)
+    roofline = {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_lo / 1e12, "unit": "Tmul/s",
+                "frac": achieved / peak_lo, "traffic": None,
+                "peak_source": "measured live: pfb_measure_int32_peak (mul.lo)",
+                "mul_hi_peak": peak_hi / 1e12,
+                "work": "%d INT32 multiplies per squaring (reference structure at %d digits)" % (ref_mults, digits)}
+
+    # --- e2e through the C ABI ---------------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        props = torch.cuda.get_device_properties(dev)
+        nb = args.e2e_batch or props.multi_processor_count
+        sub = cands[:nb]
+        barrier()
+        t0 = time.perf_counter()
+        ver, res = eng.test(sub, 2, residues=True)
+        torch.cuda.synchronize()
+        dt = max_over_ranks(time.perf_counter() - t0)
+        h2d = sum(2 * ((N.bit_length() + 15) // 16) for N in sub)
+        d2h = len(sub) + sum(2 * ((N.bit_length() + 15) // 16) for N in sub)
+        e2e = {"value": len(sub) / dt * world, "unit": "tests/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "candidates": len(sub), "seconds": dt,
+               "verdicts": {"probable_prime": int(sum(1 for v in ver if v == 1)), "composite":
+                            int(sum(1 for v in ver if v == 0))}}
+
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": "MR base-2 tests/s, 50 000-digit batch (config 3), served/batched",
+        "value": tests_s, "unit": "tests/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u32", "data": "synthetic",
+        "config": {"workload": "uniform MR batch: 256 x 50 000-digit N/rev(N), (k,j) from the "
+                               "(50000,30000,100) sieve survivors, splitmix64 seed 1",
+                   "candidates": n, "squarings_per_step": chunk, "squarings_per_test": sq_per_test,
+                   "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
+        "plain": {"value": plain_tests_s, "unit": "tests/s", "form": "one candidate per call"},
+        "served_over_plain": tests_s / world / plain_tests_s,
+        "sieve": {"value": sieve_pairs_s, "unit": "pairs/s", "K": K, "triples_per_step": ntr,
+                  "dropin_100x100_s": dropin_s, "dropin_timing": {"upload": t.upload, "kernel": t.kernel,
+                                                                  "download": t.download}},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "cpu_baseline_sieve": cpu_sieve,
+        "clocks": clocks.summary(),
+        "e2e": e2e,
+        "gpu_launches": args.steps * launches_per_step,
+    }
+    print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -26,8 +26,9 @@
 extern "C" {
 #endif
 
-/* Largest modulus: R = 2^(22*H), H = 2^13 limbs, minus the 36-bit margin. */
-#define PFB_MR_MAX_BITS (22 * 8192 - 36)
+/* Largest modulus: R = 2^(22*H), H = 2^14 limbs, minus a 36-bit margin
+ * (108 495 decimal digits). */
+#define PFB_MR_MAX_BITS (22 * 16384 - 36)
 
 typedef struct pfb_mr pfb_mr_t;
 
@@ -63,9 +64,35 @@ int pfb_mr_test(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,
 int pfb_mr_powm(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,
                 const pfb_mr_number_t *exps, uint16_t *residue, int residue_stride);
 
+/*
+ * Resident batches: the same tests as pfb_mr_test, driven step by step (the
+ * job of BatchModCtx + the witness loop, batch_mod_ctx.cuh:101-228 and
+ * miller_rabin_runner.cu:281-359, with the candidates' state kept in device
+ * memory between calls).  A step is one modular squaring of every unfinished
+ * candidate (or one verdict check).
+ *   create   host set-up, upload and transforms of N and N' (synchronous)
+ *   advance  enqueue `steps` steps on `stream` (NULL = engine stream)
+ *   pending  number of unfinished candidates (synchronises the device)
+ *   results  verdicts / residues as in pfb_mr_test; PFB_E_STATE while some
+ *            candidate is unfinished (its verdict is reported as -2)
+ */
+typedef struct pfb_mr_batch pfb_mr_batch_t;
+int pfb_mr_batch_create(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,
+                        pfb_mr_batch_t **out);
+int pfb_mr_batch_advance(pfb_mr_batch_t *b, int steps, void *stream);
+int pfb_mr_batch_pending(pfb_mr_batch_t *b, int *pending);
+long long pfb_mr_batch_steps_left(pfb_mr_batch_t *b);
+int pfb_mr_batch_results(pfb_mr_batch_t *b, int8_t *verdict, uint16_t *residue, int residue_stride);
+void pfb_mr_batch_destroy(pfb_mr_batch_t *b);
+
 /* Squarings (plus the final conversion) a strong test of N costs: the unit of
  * the engine's throughput counters. */
 long long pfb_mr_test_cost(const uint16_t *limbs, int n_limbs);
+
+/* Sustained 32-bit integer multiply rate of the device (ops/s), for the
+ * low-half and high-half forms: the roofline denominator of the squaring
+ * kernel.  No counterpart in the reference (a measurement utility). */
+int pfb_measure_int32_peak(int device, double *mul_lo_per_s, double *mul_hi_per_s);
 
 #ifdef __cplusplus
 }

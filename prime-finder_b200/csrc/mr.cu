@@ -31,6 +31,9 @@ struct JobDev {
     const uint32_t *npl;  // H limbs of N' (set-up input)
     const uint32_t *nl;   // H limbs of N
     const uint32_t *exp;  // exponent, 32-bit words, little-endian
+    uint32_t *spill_s;    // L words  (sequential-prime step only)
+    uint32_t *spill_t;    // H words  (sequential-prime step only)
+    uint32_t *ybuf;       // H words  (sequential-prime step only: canonical residue)
     int logl;
     int cursor;   // next exponent bit (MSB first); phase 0 while >= 0
     int extra;    // squarings left in phase 2 (s - 1 for a strong test)
@@ -41,21 +44,29 @@ struct JobDev {
     int steps;    // steps taken (diagnostics)
 };
 
+// Shared memory: both primes' transforms + X + Y up to L = 2^LOG_LCTA; one
+// transform + X above (the sequential-prime step keeps Y in global memory).
 __host__ __device__ inline size_t smem_words(int logl) {
     const size_t L = (size_t)1 << logl, H = L / 2;
-    return 2 * (L + L / 32) + 2 * H;
+    return logl <= LOG_LCTA ? 2 * (L + L / 32) + 2 * H : (L + L / 32) + H;
 }
 inline size_t smem_bytes(int logl) {
     return smem_words(logl) * sizeof(uint32_t) + sizeof(CarrySmem) + 16;
 }
 
-__device__ __forceinline__ void carve(uint32_t *raw, int logl, Smem &sm, uint32_t *&Y) {
+__device__ __forceinline__ void carve(uint32_t *raw, int logl, Smem &sm, uint32_t *&Y, uint32_t *ybuf) {
     const int L = 1 << logl, H = L >> 1;
     sm.A0 = raw;
-    sm.A1 = raw + L + L / 32;
-    sm.X = sm.A1 + L + L / 32;
-    Y = sm.X + H;
-    uintptr_t c = (uintptr_t)(Y + H);
+    if (logl <= LOG_LCTA) {
+        sm.A1 = raw + L + L / 32;
+        sm.X = sm.A1 + L + L / 32;
+        Y = sm.X + H;
+    } else {
+        sm.A1 = nullptr;
+        sm.X = raw + L + L / 32;
+        Y = ybuf;
+    }
+    uintptr_t c = (uintptr_t)(raw + smem_words(logl));
     c = (c + 15) & ~(uintptr_t)15;
     sm.cs = (CarrySmem *)c;
 }
@@ -66,40 +77,71 @@ __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, Twiddles
     if (jb.phase == 3) return;
     Smem sm;
     uint32_t *Y;
-    carve(raw, jb.logl, sm, Y);
+    carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int L = 1 << jb.logl, H = L >> 1;
-    for (int i = threadIdx.x; i < L; i += blockDim.x) {
-        const uint32_t v = i < H ? jb.npl[i] : 0u;
-        sm.A0[pad(i)] = v;
-        sm.A1[pad(i)] = v;
+    if (jb.logl <= LOG_LCTA) {
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            const uint32_t v = i < H ? jb.npl[i] : 0u;
+            sm.A0[pad(i)] = v;
+            sm.A1[pad(i)] = v;
+        }
+        __syncthreads();
+        dif(sm.A0, sm.A1, jb.logl, tw);
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            jb.nph[i] = red2(sm.A0[pad(i)], P1);
+            jb.nph[L + i] = red2(sm.A1[pad(i)], P2);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < H; i += blockDim.x) {
+            sm.A0[pad(i)] = jb.nl[i];
+            sm.A1[pad(i)] = jb.nl[i];
+        }
+        __syncthreads();
+        dif(sm.A0, sm.A1, jb.logl - 1, tw);
+        for (int i = threadIdx.x; i < H; i += blockDim.x) {
+            jb.nh[i] = red2(sm.A0[pad(i)], P1);
+            jb.nh[H + i] = red2(sm.A1[pad(i)], P2);
+        }
+        return;
     }
-    __syncthreads();
-    dif(sm.A0, sm.A1, jb.logl, tw);
-    for (int i = threadIdx.x; i < L; i += blockDim.x) {
-        jb.nph[i] = red2(sm.A0[pad(i)], P1);
-        jb.nph[L + i] = red2(sm.A1[pad(i)], P2);
+    uint32_t *A = sm.A0;
+    for (int pr = 0; pr < 2; pr++) {
+        for (int i = threadIdx.x; i < L; i += blockDim.x) A[pad(i)] = i < H ? jb.npl[i] : 0u;
+        __syncthreads();
+        if (pr == 0) dif1<0>(A, jb.logl, tw.w[0], tw.wsh[0]);
+        else dif1<1>(A, jb.logl, tw.w[1], tw.wsh[1]);
+        const uint32_t p = pr ? P2 : P1;
+        for (int i = threadIdx.x; i < L; i += blockDim.x) jb.nph[pr * L + i] = red2(A[pad(i)], p);
+        __syncthreads();
+        for (int i = threadIdx.x; i < H; i += blockDim.x) A[pad(i)] = jb.nl[i];
+        __syncthreads();
+        if (pr == 0) dif1<0>(A, jb.logl - 1, tw.w[0], tw.wsh[0]);
+        else dif1<1>(A, jb.logl - 1, tw.w[1], tw.wsh[1]);
+        for (int i = threadIdx.x; i < H; i += blockDim.x) jb.nh[pr * H + i] = red2(A[pad(i)], p);
+        __syncthreads();
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < H; i += blockDim.x) {
-        sm.A0[pad(i)] = jb.nl[i];
-        sm.A1[pad(i)] = jb.nl[i];
-    }
-    __syncthreads();
-    dif(sm.A0, sm.A1, jb.logl - 1, tw);
-    for (int i = threadIdx.x; i < H; i += blockDim.x) {
-        jb.nh[i] = red2(sm.A0[pad(i)], P1);
-        jb.nh[H + i] = red2(sm.A1[pad(i)], P2);
+}
+
+// One Montgomery step in the layout chosen by the transform length.
+__device__ __forceinline__ void mstep(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
+                                      const JobDev &jb) {
+    if (cd.logl <= LOG_LCTA) {
+        mont_step(sm, cd, square, a, tw, c_crt);
+    } else {
+        const Spill sp{jb.spill_s, jb.spill_t};
+        mont_step_seq(sm, cd, square, a, tw, c_crt, sp);
     }
 }
 
 // Canonical residue of X (Montgomery form) into Y: Y = X R^-1 mod N.
-__device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uint32_t *nl, const Twiddles &tw) {
+__device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uint32_t *nl, const Twiddles &tw,
+                          const JobDev &jb) {
     const int H = 1 << (cd.logl - 1);
     for (int i = threadIdx.x; i < H; i += blockDim.x) Y[i] = sm.X[i];
     __syncthreads();
     Smem s2 = sm;
     s2.X = Y;
-    mont_step(s2, cd, false, 1u, tw, c_crt);
+    mstep(s2, cd, false, 1u, tw, jb);
     // REDC(X) lies in [0, N]; it is N only when X == 0 (mod N), e.g. a base
     // that is a multiple of N.  Map it to 0.
     bool eqn = true;
@@ -116,7 +158,7 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel(JobDev *jobs, int max_
     if (jb.phase == 3) return;
     Smem sm;
     uint32_t *Y;
-    carve(raw, jb.logl, sm, Y);
+    carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int H = 1 << (jb.logl - 1);
     const Cand cd{jb.nph, jb.nh, jb.logl};
     for (int i = threadIdx.x; i < H; i += blockDim.x) sm.X[i] = jb.x[i];
@@ -126,15 +168,15 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel(JobDev *jobs, int max_
     while (steps < max_steps && phase != 3) {
         if (phase == 0) {
             const uint32_t bit = (__ldg(jb.exp + (cursor >> 5)) >> (cursor & 31)) & 1u;
-            mont_step(sm, cd, true, bit ? jb.base : 1u, tw, c_crt);
+            mstep(sm, cd, true, bit ? jb.base : 1u, tw, jb);
             cursor--;
             if (cursor < 0) phase = 1;
         } else {
             if (phase == 2) {
-                mont_step(sm, cd, true, 1u, tw, c_crt);
+                mstep(sm, cd, true, 1u, tw, jb);
                 extra--;
             }
-            canonical(sm, Y, cd, jb.nl, tw);
+            canonical(sm, Y, cd, jb.nl, tw, jb);
             // compare with 1 and N - 1 (N odd: N - 1 differs from N in limb 0 only)
             bool one = true, nm1 = true;
             for (int i = threadIdx.x; i < H; i += blockDim.x) {
@@ -195,7 +237,7 @@ struct HostPrep {
 
 static int choose_logl(size_t nbits, uint32_t base) {
     const int abits = 32 - __builtin_clz(base);
-    for (int lg = LOG_LMIN; lg <= LOG_LCTA; lg++) {
+    for (int lg = LOG_LMIN; lg <= LOG_LSEQ; lg++) {
         const size_t rbits = (size_t)LIMB_BITS << (lg - 1);
         if (rbits >= nbits + 2 + 2 * (size_t)abits) return lg;
     }
@@ -254,8 +296,6 @@ struct pfb_mr {
     cudaStream_t stream = nullptr;
     uint32_t *d_tw = nullptr;
     Twiddles tw{};
-    uint8_t *d_arena = nullptr;
-    size_t arena_bytes = 0;
 };
 
 static int build_tables(pfb_mr *e) {
@@ -329,7 +369,7 @@ extern "C" int pfb_mr_create(pfb_mr_t **out, int device) {
     }
     if (!rc) rc = build_tables(e);
     if (!rc) {
-        const int mx = (int)smem_bytes(LOG_LCTA);
+        const int mx = (int)std::max(smem_bytes(LOG_LCTA), smem_bytes(LOG_LSEQ));
         ce = cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         if (ce == cudaSuccess) ce = cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "smem attribute", __FILE__, __LINE__);
@@ -352,7 +392,6 @@ extern "C" void pfb_mr_destroy(pfb_mr_t *e) {
         cudaStreamDestroy(e->stream);
     }
     cudaFree(e->d_tw);
-    cudaFree(e->d_arena);
     delete e;
 }
 
@@ -360,7 +399,7 @@ namespace {
 
 // Per-candidate device layout inside the arena (32-bit words).
 struct Layout {
-    size_t x, res, nph, nh, npl, nl, exp, total;
+    size_t x, res, nph, nh, npl, nl, exp, ss, st, yb, total;
 };
 
 Layout layout_for(const HostPrep &hp) {
@@ -379,6 +418,11 @@ Layout layout_for(const HostPrep &hp) {
     l.npl = take(H);
     l.nl = take(H);
     l.exp = take(hp.exp.size());
+    if (hp.logl > LOG_LCTA) {
+        l.ss = take(L);
+        l.st = take(H);
+        l.yb = take(H);
+    }
     l.total = o;
     return l;
 }
@@ -400,109 +444,177 @@ void prep_all(const pfb_mr_number_t *nums, int n, uint32_t base, int mode, const
     for (auto &x : th) x.join();
 }
 
-int run_jobs(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int mode,
-             const pfb_mr_number_t *exps, int8_t *verdict, uint16_t *residue, int residue_stride) {
+}  // namespace
+
+// A set of candidates resident in device memory, advanced step by step.
+struct pfb_mr_batch {
+    pfb_mr *e = nullptr;
+    int n = 0, mode = 1, maxlog = LOG_LMIN, n_ok = 0;
+    long long max_steps = 0, steps_done = 0;
+    uint8_t *d_arena = nullptr;
+    JobDev *d_jobs = nullptr;
+    std::vector<HostPrep> hp;
+    std::vector<JobDev> jobs;
+};
+
+namespace {
+
+int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int mode,
+                const pfb_mr_number_t *exps, pfb_mr_batch **out) {
+    *out = nullptr;
     if (!e || !nums || n <= 0 || base < 2 || base > 0xFFFFu) {
         pfb::set_error("pfb_mr: bad argument (n=%d base=%u)", n, base);
         return PFB_E_ARG;
     }
-    if (residue && residue_stride <= 0) {
-        pfb::set_error("pfb_mr: residue_stride must be > 0");
-        return PFB_E_ARG;
-    }
     PFB_CUDA(cudaSetDevice(e->device));
-    std::vector<HostPrep> hp;
-    prep_all(nums, n, base, mode, exps, hp);
+    pfb_mr_batch *b = new pfb_mr_batch();
+    b->e = e;
+    b->n = n;
+    b->mode = mode;
+    prep_all(nums, n, base, mode, exps, b->hp);
     std::vector<Layout> lay(n);
     size_t total = 0;
-    int maxlog = LOG_LMIN, n_ok = 0;
-    long long max_steps = 0;
     for (int i = 0; i < n; i++) {
-        if (verdict) verdict[i] = -1;
-        if (!hp[i].ok) continue;
-        lay[i] = layout_for(hp[i]);
+        if (!b->hp[i].ok) continue;
+        lay[i] = layout_for(b->hp[i]);
         total += lay[i].total;
-        maxlog = std::max(maxlog, hp[i].logl);
-        max_steps = std::max(max_steps, (long long)hp[i].cursor + 2 + hp[i].s);
-        n_ok++;
+        b->maxlog = std::max(b->maxlog, b->hp[i].logl);
+        b->max_steps = std::max(b->max_steps, (long long)b->hp[i].cursor + 2 + b->hp[i].s);
+        b->n_ok++;
     }
     const size_t job_bytes = ((size_t)n * sizeof(JobDev) + 255) & ~(size_t)255;
     const size_t need = job_bytes + total * sizeof(uint32_t);
-    if (need > e->arena_bytes) {
-        cudaFree(e->d_arena);
-        e->d_arena = nullptr;
-        e->arena_bytes = 0;
-        cudaError_t ce = cudaMalloc(&e->d_arena, need);
-        if (ce != cudaSuccess) {
-            pfb::set_error("pfb_mr: cannot allocate %zu bytes", need);
-            return PFB_E_NOMEM;
-        }
-        e->arena_bytes = need;
+    if (cudaMalloc(&b->d_arena, need) != cudaSuccess) {
+        cudaGetLastError();
+        pfb::set_error("pfb_mr: cannot allocate %zu bytes of device memory", need);
+        delete b;
+        return PFB_E_NOMEM;
     }
-    JobDev *d_jobs = (JobDev *)e->d_arena;
-    uint32_t *d_words = (uint32_t *)(e->d_arena + job_bytes);
-    std::vector<JobDev> jobs(n);
+    b->d_jobs = (JobDev *)b->d_arena;
+    uint32_t *d_words = (uint32_t *)(b->d_arena + job_bytes);
+    b->jobs.assign(n, JobDev{});
     size_t off = 0;
-    for (int i = 0; i < n; i++) {
-        JobDev &j = jobs[i];
+    int rc = PFB_OK;
+    for (int i = 0; i < n && !rc; i++) {
+        JobDev &j = b->jobs[i];
         memset(&j, 0, sizeof(j));
-        if (!hp[i].ok) {
+        const HostPrep &h = b->hp[i];
+        if (!h.ok) {
             j.phase = 3;
+            j.verdict = -1;
             continue;
         }
-        uint32_t *b = d_words + off;
+        uint32_t *w = d_words + off;
         const Layout &l = lay[i];
-        j.x = b + l.x;
-        j.res = b + l.res;
-        j.nph = b + l.nph;
-        j.nh = b + l.nh;
-        j.npl = b + l.npl;
-        j.nl = b + l.nl;
-        j.exp = b + l.exp;
-        j.logl = hp[i].logl;
-        j.cursor = hp[i].cursor;
-        j.extra = mode == 1 ? hp[i].s - 1 : 0;
+        j.x = w + l.x;
+        j.res = w + l.res;
+        j.nph = w + l.nph;
+        j.nh = w + l.nh;
+        j.npl = w + l.npl;
+        j.nl = w + l.nl;
+        j.exp = w + l.exp;
+        if (h.logl > LOG_LCTA) {
+            j.spill_s = w + l.ss;
+            j.spill_t = w + l.st;
+            j.ybuf = w + l.yb;
+        }
+        j.logl = h.logl;
+        j.cursor = h.cursor;
+        j.extra = mode == 1 ? h.s - 1 : 0;
         j.phase = 0;
         j.base = base;
         j.mode = mode;
-        const size_t H = hp[i].x0.size();
-        PFB_CUDA(cudaMemcpyAsync(j.x, hp[i].x0.data(), H * 4, cudaMemcpyHostToDevice, e->stream));
-        PFB_CUDA(cudaMemcpyAsync((void *)j.npl, hp[i].npl.data(), H * 4, cudaMemcpyHostToDevice, e->stream));
-        PFB_CUDA(cudaMemcpyAsync((void *)j.nl, hp[i].nl.data(), H * 4, cudaMemcpyHostToDevice, e->stream));
-        PFB_CUDA(cudaMemcpyAsync((void *)j.exp, hp[i].exp.data(), hp[i].exp.size() * 4, cudaMemcpyHostToDevice,
-                                 e->stream));
+        const size_t H = h.x0.size();
+        cudaError_t ce = cudaMemcpyAsync(j.x, h.x0.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync((void *)j.npl, h.npl.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync((void *)j.nl, h.nl.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync((void *)j.exp, h.exp.data(), h.exp.size() * 4, cudaMemcpyHostToDevice, e->stream);
+        if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "batch upload", __FILE__, __LINE__);
         off += l.total;
     }
-    PFB_CUDA(cudaMemcpyAsync(d_jobs, jobs.data(), n * sizeof(JobDev), cudaMemcpyHostToDevice, e->stream));
-    if (n_ok) {
-        const size_t sm = smem_bytes(maxlog);
-        prep_kernel<<<n, THREADS, sm, e->stream>>>(d_jobs, e->tw);
-        PFB_CUDA(cudaGetLastError());
-        const int chunk = 2048;
-        for (long long done = 0; done < max_steps; done += chunk) {
-            step_kernel<<<n, THREADS, sm, e->stream>>>(d_jobs, chunk, e->tw);
-            PFB_CUDA(cudaGetLastError());
-        }
+    cudaError_t ce = cudaSuccess;
+    if (!rc) ce = cudaMemcpyAsync(b->d_jobs, b->jobs.data(), n * sizeof(JobDev), cudaMemcpyHostToDevice, e->stream);
+    if (!rc && ce != cudaSuccess) rc = pfb::cuda_fail(ce, "job upload", __FILE__, __LINE__);
+    if (!rc && b->n_ok) {
+        prep_kernel<<<n, THREADS, smem_bytes(b->maxlog), e->stream>>>(b->d_jobs, e->tw);
+        ce = cudaGetLastError();
+        if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "prep_kernel", __FILE__, __LINE__);
     }
-    PFB_CUDA(cudaMemcpyAsync(jobs.data(), d_jobs, n * sizeof(JobDev), cudaMemcpyDeviceToHost, e->stream));
+    // host staging must outlive the copies; later work may use other streams
+    if (!rc) {
+        ce = cudaStreamSynchronize(e->stream);
+        if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "batch sync", __FILE__, __LINE__);
+    }
+    if (rc) {
+        cudaFree(b->d_arena);
+        delete b;
+        return rc;
+    }
+    *out = b;
+    return PFB_OK;
+}
+
+int batch_advance(pfb_mr_batch *b, long long steps, cudaStream_t st) {
+    if (!b->n_ok) return PFB_OK;
+    const size_t sm = smem_bytes(b->maxlog);
+    const int chunk = 2048;
+    while (steps > 0) {
+        const int k = (int)std::min<long long>(steps, chunk);
+        step_kernel<<<b->n, THREADS, sm, st>>>(b->d_jobs, k, b->e->tw);
+        PFB_CUDA(cudaGetLastError());
+        steps -= k;
+        b->steps_done += k;
+    }
+    return PFB_OK;
+}
+
+int batch_results(pfb_mr_batch *b, int8_t *verdict, uint16_t *residue, int residue_stride) {
+    pfb_mr *e = b->e;
+    PFB_CUDA(cudaMemcpyAsync(b->jobs.data(), b->d_jobs, b->n * sizeof(JobDev), cudaMemcpyDeviceToHost, e->stream));
     PFB_CUDA(cudaStreamSynchronize(e->stream));
     std::vector<uint32_t> r22;
-    for (int i = 0; i < n; i++) {
-        if (!hp[i].ok) continue;
-        if (jobs[i].phase != 3) {
-            pfb::set_error("pfb_mr: candidate %d did not finish", i);
-            return PFB_E_STATE;
+    int rc = PFB_OK;
+    for (int i = 0; i < b->n; i++) {
+        const JobDev &j = b->jobs[i];
+        if (!b->hp[i].ok) {
+            if (verdict) verdict[i] = -1;
+            if (residue) memset(residue + (size_t)i * residue_stride, 0, sizeof(uint16_t) * residue_stride);
+            continue;
         }
-        if (verdict) verdict[i] = (int8_t)(mode == 1 ? jobs[i].verdict : 0);
+        if (j.phase != 3) {
+            if (verdict) verdict[i] = -2;
+            rc = PFB_E_STATE;
+            continue;
+        }
+        if (verdict) verdict[i] = (int8_t)(b->mode == 1 ? j.verdict : 0);
         if (residue) {
-            const size_t H = hp[i].x0.size();
+            const size_t H = b->hp[i].x0.size();
             r22.resize(H);
-            PFB_CUDA(cudaMemcpy(r22.data(), jobs[i].res, H * 4, cudaMemcpyDeviceToHost));
+            PFB_CUDA(cudaMemcpy(r22.data(), j.res, H * 4, cudaMemcpyDeviceToHost));
             pfb::big::Words r = pfb::big::from_limbs(r22.data(), LIMB_BITS, H);
             pfb::big::to_u16(r, residue + (size_t)i * residue_stride, (size_t)residue_stride);
         }
     }
-    return PFB_OK;
+    if (rc) pfb::set_error("pfb_mr: some candidates have not finished");
+    return rc;
+}
+
+int run_jobs(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int mode,
+             const pfb_mr_number_t *exps, int8_t *verdict, uint16_t *residue, int residue_stride) {
+    if (residue && residue_stride <= 0) {
+        pfb::set_error("pfb_mr: residue_stride must be > 0");
+        return PFB_E_ARG;
+    }
+    pfb_mr_batch *b = nullptr;
+    int rc = batch_build(e, nums, n, base, mode, exps, &b);
+    if (rc) return rc;
+    rc = batch_advance(b, b->max_steps, e->stream);
+    if (!rc) rc = batch_results(b, verdict, residue, residue_stride);
+    cudaStreamSynchronize(e->stream);
+    cudaFree(b->d_arena);
+    delete b;
+    return rc;
 }
 
 }  // namespace
@@ -519,6 +631,61 @@ extern "C" int pfb_mr_powm(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint
         return PFB_E_ARG;
     }
     return run_jobs(e, nums, n, base, 0, exps, nullptr, residue, residue_stride);
+}
+
+extern "C" int pfb_mr_batch_create(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,
+                                   pfb_mr_batch_t **out) {
+    if (!out) {
+        pfb::set_error("pfb_mr_batch_create: null out");
+        return PFB_E_ARG;
+    }
+    return batch_build(e, nums, n, base, 1, nullptr, out);
+}
+
+extern "C" int pfb_mr_batch_advance(pfb_mr_batch_t *b, int steps, void *stream) {
+    if (!b || steps < 0) {
+        pfb::set_error("pfb_mr_batch_advance: bad argument");
+        return PFB_E_ARG;
+    }
+    PFB_CUDA(cudaSetDevice(b->e->device));
+    return batch_advance(b, steps, stream ? (cudaStream_t)stream : b->e->stream);
+}
+
+extern "C" int pfb_mr_batch_pending(pfb_mr_batch_t *b, int *pending) {
+    if (!b || !pending) {
+        pfb::set_error("pfb_mr_batch_pending: bad argument");
+        return PFB_E_ARG;
+    }
+    PFB_CUDA(cudaSetDevice(b->e->device));
+    PFB_CUDA(cudaDeviceSynchronize());
+    PFB_CUDA(cudaMemcpy(b->jobs.data(), b->d_jobs, b->n * sizeof(JobDev), cudaMemcpyDeviceToHost));
+    int c = 0;
+    for (int i = 0; i < b->n; i++) c += b->jobs[i].phase != 3;
+    *pending = c;
+    return PFB_OK;
+}
+
+extern "C" long long pfb_mr_batch_steps_left(pfb_mr_batch_t *b) {
+    if (!b) return -1;
+    return std::max(0ll, b->max_steps - b->steps_done);
+}
+
+extern "C" int pfb_mr_batch_results(pfb_mr_batch_t *b, int8_t *verdict, uint16_t *residue, int residue_stride) {
+    if (!b || (residue && residue_stride <= 0)) {
+        pfb::set_error("pfb_mr_batch_results: bad argument");
+        return PFB_E_ARG;
+    }
+    PFB_CUDA(cudaSetDevice(b->e->device));
+    PFB_CUDA(cudaDeviceSynchronize());
+    return batch_results(b, verdict, residue, residue_stride);
+}
+
+extern "C" void pfb_mr_batch_destroy(pfb_mr_batch_t *b) {
+    if (!b) return;
+    cudaSetDevice(b->e->device);
+    cudaDeviceSynchronize();
+    cudaFree(b->d_arena);
+    delete b;
 }
 
 extern "C" long long pfb_mr_test_cost(const uint16_t *limbs, int n_limbs) {

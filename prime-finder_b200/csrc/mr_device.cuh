@@ -29,6 +29,7 @@ constexpr uint32_t LIMB_MASK = (1u << LIMB_BITS) - 1u;
 constexpr int LOG_LMAX = 15;          // twiddle tables cover L <= 2^15
 constexpr int LOG_LMIN = 8;
 constexpr int LOG_LCTA = 14;          // largest L whose two transforms fit one CTA
+constexpr int LOG_LSEQ = 15;          // largest L of the sequential-prime step
 constexpr int THREADS = 512;
 
 // Twiddles: w[p][k] = omega^k, omega of order 2^LOG_LMAX, k < 2^(LOG_LMAX-1);
@@ -241,6 +242,51 @@ __device__ void dit(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
     }
 }
 
+// Single-prime transforms: all threads of the CTA work on prime PR.
+template <int PR>
+__device__ void dif1(uint32_t *A, int logn, const uint32_t *W, const uint32_t *Wsh) {
+    int s = logn, h0 = 1 << (logn - 1);
+    const int g0 = threadIdx.x, st = blockDim.x;
+    while (s > 0) {
+        if (s >= 4) {
+            dif_pass1<PR, 4>(A, logn, h0, W, Wsh, g0, st);
+            h0 >>= 4;
+            s -= 4;
+        } else if (s == 3) {
+            dif_pass1<PR, 3>(A, logn, h0, W, Wsh, g0, st);
+            s = 0;
+        } else if (s == 2) {
+            dif_pass1<PR, 2>(A, logn, h0, W, Wsh, g0, st);
+            s = 0;
+        } else {
+            dif_pass1<PR, 1>(A, logn, h0, W, Wsh, g0, st);
+            s = 0;
+        }
+        __syncthreads();
+    }
+}
+
+template <int PR>
+__device__ void dit1(uint32_t *A, int logn, const uint32_t *W, const uint32_t *Wsh) {
+    int s = logn, h0 = 1;
+    const int g0 = threadIdx.x, st = blockDim.x;
+    const int r0 = logn & 3;
+    if (r0) {
+        if (r0 == 3) dit_pass1<PR, 3>(A, logn, h0, W, Wsh, g0, st);
+        else if (r0 == 2) dit_pass1<PR, 2>(A, logn, h0, W, Wsh, g0, st);
+        else dit_pass1<PR, 1>(A, logn, h0, W, Wsh, g0, st);
+        h0 <<= r0;
+        s -= r0;
+        __syncthreads();
+    }
+    while (s > 0) {
+        dit_pass1<PR, 4>(A, logn, h0, W, Wsh, g0, st);
+        h0 <<= 4;
+        s -= 4;
+        __syncthreads();
+    }
+}
+
 // Scratch of the carry-lookahead scan.
 struct CarrySmem {
     unsigned long long wc[THREADS / 32];
@@ -429,6 +475,94 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
     if (a > 1u) {
         carry_pass<false>(H, 0ull, [&](int i) { return (unsigned long long)X[i] * a; }, X, cs);
     }
+}
+
+// Global scratch of the sequential-prime step (one per resident candidate).
+struct Spill {
+    uint32_t *s;   // L words: prime-1 inverse transform, read back by the CRT
+    uint32_t *t;   // H words: T mod R, then m
+};
+
+__device__ __forceinline__ uint32_t ldg_spill(const uint32_t *p) { return __ldcg(p); }
+
+// mont_step for transforms too long for both primes to sit in shared memory
+// (L = 2^15): the p1 spectrum makes a round trip through global memory (L2).
+// Same arithmetic and result as mont_step; sm.A1 is unused.
+__device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
+                              const CrtConsts &cc, const Spill &sp) {
+    const int logl = cd.logl, L = 1 << logl, H = L >> 1;
+    uint32_t *A = sm.A0, *X = sm.X;
+    CarrySmem &cs = *sm.cs;
+    const int tid = threadIdx.x, T = blockDim.x;
+    unsigned long long cS = 0;
+    auto load_x = [&](const uint32_t *src, bool from_global) {
+        for (int i = tid; i < L; i += T) A[pad(i)] = i < H ? (from_global ? ldg_spill(src + i) : src[i]) : 0u;
+        __syncthreads();
+    };
+    auto spill = [&](int n) {
+        for (int i = tid; i < n; i += T) sp.s[i] = A[pad(i)];
+        __syncthreads();
+    };
+    if (square) {
+        load_x(X, false);
+        dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
+        for (int i = tid; i < L; i += T) {
+            const uint32_t u = A[pad(i)];
+            A[pad(i)] = mont(u, u, P1, cc.pinv[0]);
+        }
+        __syncthreads();
+        dit1<0>(A, logl, tw.wi[0], tw.wish[0]);
+        spill(L);
+        load_x(X, false);
+        dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
+        for (int i = tid; i < L; i += T) {
+            const uint32_t u = A[pad(i)];
+            A[pad(i)] = mont(u, u, P2, cc.pinv[1]);
+        }
+        __syncthreads();
+        dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
+        carry_pass<true>(L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
+        cS = carry_pass<false>(H, 0ull,
+                               [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
+        for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
+        for (int i = H + tid; i < L; i += T) A[pad(i)] = 0u;
+        __syncthreads();
+    } else {
+        for (int i = tid; i < H; i += T) sp.t[i] = X[i];
+        load_x(X, false);
+    }
+    // m = T_lo * N' mod R
+    dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
+    for (int i = tid; i < L; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nph + i), P1, cc.pinv[0]);
+    __syncthreads();
+    dit1<0>(A, logl, tw.wi[0], tw.wish[0]);
+    spill(H);
+    load_x(sp.t, true);
+    dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
+    for (int i = tid; i < L; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nph + L + i), P2, cc.pinv[1]);
+    __syncthreads();
+    dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
+    carry_pass<true>(H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
+    for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
+    __syncthreads();
+    // W = m * N mod (R - 1)
+    dif1<0>(A, logl - 1, tw.w[0], tw.wsh[0]);
+    for (int i = tid; i < H; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nh + i), P1, cc.pinv[0]);
+    __syncthreads();
+    dit1<0>(A, logl - 1, tw.wi[0], tw.wish[0]);
+    spill(H);
+    for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
+    __syncthreads();
+    dif1<1>(A, logl - 1, tw.w[1], tw.wsh[1]);
+    for (int i = tid; i < H; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nh + H + i), P2, cc.pinv[1]);
+    __syncthreads();
+    dit1<1>(A, logl - 1, tw.wi[1], tw.wish[1]);
+    const unsigned long long cW = carry_pass<true>(
+        H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl - 1, cc); }, A, cs);
+    unsigned long long c = carry_pass<false>(
+        H, cS + cW, [&](int i) { return (unsigned long long)X[i] + A[pad(i)]; }, X, cs);
+    while (c) c = carry_pass<false>(H, c, [&](int i) { return (unsigned long long)X[i]; }, X, cs);
+    if (a > 1u) carry_pass<false>(H, 0ull, [&](int i) { return (unsigned long long)X[i] * a; }, X, cs);
 }
 
 }  // namespace mr

@@ -207,7 +207,7 @@ def unpack_mask(mask: np.ndarray, K: int) -> np.ndarray:
 
 # ------------------------------------------------------------ Miller-Rabin ---
 
-MR_MAX_BITS = 22 * 8192 - 36
+MR_MAX_BITS = 22 * 16384 - 36
 
 
 class _Number(C.Structure):
@@ -301,3 +301,100 @@ class MillerRabin:
                                    res.ctypes.data_as(C.POINTER(C.c_uint16)), stride)
         _check(rc, "pfb_mr_powm")
         return [limbs16_to_int(res[i * stride:(i + 1) * stride]) for i in range(n)]
+
+
+def _batch_lib():
+    L = _mr_lib()
+    if not hasattr(L, "_batch_ready"):
+        vp = C.c_void_p
+        L.pfb_mr_batch_create.argtypes = [vp, C.POINTER(_Number), C.c_int, C.c_uint32, C.POINTER(vp)]
+        L.pfb_mr_batch_create.restype = C.c_int
+        L.pfb_mr_batch_advance.argtypes = [vp, C.c_int, vp]
+        L.pfb_mr_batch_advance.restype = C.c_int
+        L.pfb_mr_batch_pending.argtypes = [vp, C.POINTER(C.c_int)]
+        L.pfb_mr_batch_pending.restype = C.c_int
+        L.pfb_mr_batch_steps_left.argtypes = [vp]
+        L.pfb_mr_batch_steps_left.restype = C.c_longlong
+        L.pfb_mr_batch_results.argtypes = [vp, C.POINTER(C.c_int8), C.POINTER(C.c_uint16), C.c_int]
+        L.pfb_mr_batch_results.restype = C.c_int
+        L.pfb_mr_batch_destroy.argtypes = [vp]
+        L.pfb_mr_batch_destroy.restype = None
+        L.pfb_measure_int32_peak.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.pfb_measure_int32_peak.restype = C.c_int
+        L._batch_ready = True
+    return L
+
+
+class MRBatch:
+    """Candidates resident on the GPU, advanced step by step (pfb_mr_batch_*)."""
+
+    def __init__(self, engine: "MillerRabin", numbers, base: int = 2):
+        L = _batch_lib()
+        st, self._keep = _numbers(numbers)
+        h = C.c_void_p()
+        _check(L.pfb_mr_batch_create(engine._h, st, len(self._keep), base, C.byref(h)),
+               "pfb_mr_batch_create")
+        self._h = h
+        self.n = len(self._keep)
+
+    def advance(self, steps: int, stream: int = 0) -> None:
+        _check(_batch_lib().pfb_mr_batch_advance(self._h, steps, stream or None), "pfb_mr_batch_advance")
+
+    def steps_left(self) -> int:
+        return int(_batch_lib().pfb_mr_batch_steps_left(self._h))
+
+    def pending(self) -> int:
+        c = C.c_int(0)
+        _check(_batch_lib().pfb_mr_batch_pending(self._h, C.byref(c)), "pfb_mr_batch_pending")
+        return int(c.value)
+
+    def results(self, residues: bool = False):
+        ver = np.zeros(self.n, dtype=np.int8)
+        stride = max(len(a) for a in self._keep)
+        res = np.zeros(self.n * stride, dtype=np.uint16) if residues else None
+        rc = _batch_lib().pfb_mr_batch_results(
+            self._h, ver.ctypes.data_as(C.POINTER(C.c_int8)),
+            res.ctypes.data_as(C.POINTER(C.c_uint16)) if residues else None, stride)
+        if rc not in (PFB_OK, PFB_E_STATE):
+            _check(rc, "pfb_mr_batch_results")
+        out = None
+        if residues:
+            out = [limbs16_to_int(res[i * stride:(i + 1) * stride]) for i in range(self.n)]
+        return ver.tolist(), out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _batch_lib().pfb_mr_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def measure_int32_peak(device: int = 0):
+    """(mul.lo ops/s, mul.hi ops/s) sustained on `device`."""
+    lo, hi = C.c_double(0), C.c_double(0)
+    _check(_batch_lib().pfb_measure_int32_peak(device, C.byref(lo), C.byref(hi)), "pfb_measure_int32_peak")
+    return lo.value, hi.value
+
+
+# ----------------------------------------------------------- candidates ---
+
+def ndigits(x: int) -> int:
+    return len(str(x))
+
+
+def rev_digits(x: int, lx: int) -> int:
+    return int(str(x).zfill(lx)[::-1])
+
+
+def build_candidate(a: int, b: int, c: int, k: int, j: int, rev: bool = False) -> int:
+    """N = 10^a - k 10^b - j 10^c - 1, or rev(N) = 10^a - rev(k) 10^(a-b-lk)
+    - rev(j) 10^(a-c-lj) - 1 (miller_rabin.c:56-99)."""
+    if rev:
+        lk, lj = ndigits(k), ndigits(j)
+        return 10 ** a - rev_digits(k, lk) * 10 ** (a - b - lk) - rev_digits(j, lj) * 10 ** (a - c - lj) - 1
+    return 10 ** a - k * 10 ** b - j * 10 ** c - 1

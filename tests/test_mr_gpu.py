@@ -119,7 +119,7 @@ def test_random_composites_and_strong_pseudoprimes(mr):
 def test_mixed_lengths_one_batch(mr):
     rng = random.Random(9)
     Ns = []
-    for bits in (40, 2700, 2760, 5800, 11000, 23000, 45000, 90000, 150000, 166096):
+    for bits in (40, 2700, 2760, 5800, 11000, 23000, 45000, 90000, 150000, 166096, 200000, 332192):
         Ns.append(rng.getrandbits(bits) | (1 << (bits - 1)) | 1)
     Es = [rng.getrandbits(64) | 1 for _ in Ns]
     got = mr.powm(Ns, Es, 2)
@@ -136,7 +136,7 @@ def test_bucket_boundaries(mr):
     # largest modulus of each transform length, and one bit more
     rng = random.Random(13)
     Ns = []
-    for lg in range(8, 15):
+    for lg in range(8, 16):
         rb = 22 * (1 << (lg - 1))
         for bits in (rb - 36, rb - 35):
             if bits <= pfb200.MR_MAX_BITS:
@@ -171,3 +171,27 @@ def test_config1_full_size_residues(mr):
             want = g["ref_miller_rabin_test"]["%d,%d" % (k, j)]
             got = 0 if ver[i] == 0 else (2 if ver[i + 1] == 1 else 1)
             assert got == want
+
+
+def test_resident_batch_stepwise_equals_one_shot(mr):
+    """Advancing a resident batch in uneven chunks gives the one-shot result
+    (state round-trips through device memory between launches)."""
+    rng = random.Random(21)
+    Ns = [rng.getrandbits(b) | (1 << (b - 1)) | 1 for b in (1200, 3000, 7000, 7001, 40000)]
+    Ns.append((1 << 1279) - 1)
+    want_v, want_r = mr.test(Ns, 3)
+    b = pfb200.MRBatch(mr, Ns, 3)
+    left = b.steps_left()
+    assert left >= 40000
+    done = 0
+    for k in (1, 7, 500, 3000):
+        b.advance(k)
+        done += k
+    assert b.pending() > 0
+    v, _ = b.results()
+    assert -2 in v  # unfinished candidates are reported, not guessed
+    b.advance(left - done)
+    assert b.pending() == 0
+    v, r = b.results(residues=True)
+    assert v == want_v and r == want_r
+    b.close()
