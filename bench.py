@@ -36,6 +36,7 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "prime-finder_b200"))
+sys.set_int_max_str_digits(0)
 
 SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference count)
 

@@ -384,6 +384,7 @@ def measure_int32_peak(device: int = 0):
 # ----------------------------------------------------------- candidates ---
 
 def ndigits(x: int) -> int:
+    """Decimal digits of a small non-negative integer (k or j)."""
     return len(str(x))
 
 
