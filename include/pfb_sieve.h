@@ -90,6 +90,26 @@ int trial_div_gpu_grid(const uint32_t *primes, uint32_t n_primes,
                        const long long *abc, int n_abc, int K, uint8_t *mask_out,
                        unsigned flags);
 
+/*
+ * Allocation-free variant of pfb_sieve_run for one triple.  No counterpart in
+ * the reference: it exists for callers that cannot call cudaMalloc (a process
+ * whose device memory is reserved up front by another allocator, or a loop
+ * that cannot take the device-wide synchronisation cudaFree implies).
+ *   d_primes  device array of n_primes odd primes (no repeated entries)
+ *   d_mask    device mask block of pfb_sieve_mask_bytes(K) bytes, written
+ *             (or OR-ed with PFB_SIEVE_OR) asynchronously on `stream`
+ * Limits: one triple per call, 1 <= K <= 9999 (PFB_E_CAPACITY otherwise).
+ * Working memory is one fixed 1.16 MB __device__ array inside the library,
+ * held by every GPU that loads it until the process exits; nothing is
+ * allocated.  All calls share that array: calls that overlap on the GPU (two
+ * streams, two host threads) race and must be serialised by the caller.  The
+ * first call on a device also looks up the array's device address and sets
+ * the tile kernel's shared-memory limit; make that first call before any
+ * stream capture.
+ */
+int pfb_sieve_run_noalloc(const uint32_t *d_primes, uint32_t n_primes, long long a, long long b,
+                          long long c, int K, uint32_t *d_mask, unsigned flags, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -25,6 +25,7 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -853,4 +854,115 @@ void trial_div_launch(const uint32_t *d_primes, uint32_t n_primes, uint64_t a, u
     if (ensure_split(s, 100)) return;
     cudaMemcpyAsync(s->d_abc, abc, sizeof(abc), cudaMemcpyHostToDevice, st);
     enqueue_sieve(s, 1, 100, d_bits, st);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point.
+//
+// Some callers cannot call cudaMalloc: a process whose device memory is
+// reserved up front by another allocator (a framework's caching allocator or
+// a fixed memory pool that owns nearly all of HBM), or a latency-sensitive
+// loop that cannot take the device-wide synchronisation cudaFree implies.
+// pfb_sieve_run_noalloc serves them: the caller passes the prime list and the
+// mask in device memory it already owns, and the working memory of the sieve
+// (small-prime lists and their counts, the per-prime line records, the
+// triple) lives in one file-scope __device__ array of fixed size that every
+// GPU loading this library holds until the process exits.
+
+namespace {
+
+constexpr uint32_t kNoAllocListCap = 10000u / 2u + 2u;  // small primes (< 10000) per list
+
+struct NoAllocScratch {
+    uint32_t counts[2];
+    uint32_t pad0[62];
+    long long abc[4];
+    uint32_t tiny[kNoAllocListCap];
+    uint32_t small[kNoAllocListCap];
+    SmallRec rec[2 * kNoAllocListCap];
+};
+
+// 1.16 MB: the scratch of one triple at any K <= 9999.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+__global__ void noalloc_begin_kernel(NoAllocScratch *sc, long long a, long long b, long long c) {
+    sc->counts[0] = 0u;
+    sc->counts[1] = 0u;
+    sc->abc[0] = a;
+    sc->abc[1] = b;
+    sc->abc[2] = c;
+}
+
+std::mutex g_noalloc_mu;
+NoAllocScratch *g_noalloc_ptr[128];
+int g_noalloc_sms[128];
+
+// Once per device, with that device current: the device address of the
+// scratch array (in host code its name is only a host-side stand-in).
+int noalloc_scratch(int dev, NoAllocScratch **out, int *sms) {
+    if (dev < 0 || dev >= 128) {
+        pfb::set_error("pfb_sieve_run_noalloc: device %d out of range", dev);
+        return PFB_E_ARG;
+    }
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void *p = nullptr;
+        PFB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        int n = 0;
+        PFB_CUDA(cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev));
+        PFB_CUDA(cudaFuncSetAttribute(small_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)tile_smem_bytes(kTileRows, PFB_SIEVE_MAX_K)));
+        g_noalloc_sms[dev] = n;
+        g_noalloc_ptr[dev] = (NoAllocScratch *)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    *sms = g_noalloc_sms[dev];
+    return PFB_OK;
+}
+
+}  // namespace
+
+extern "C" int pfb_sieve_run_noalloc(const uint32_t *d_primes, uint32_t n_primes, long long a, long long b,
+                                     long long c, int K, uint32_t *d_mask, unsigned flags, void *stream) {
+    if ((n_primes && !d_primes) || !d_mask || a < 0 || b < 0 || c < 0) {
+        pfb::set_error("pfb_sieve_run_noalloc: bad argument");
+        return PFB_E_ARG;
+    }
+    if (K < 1 || K > PFB_SIEVE_MAX_K) {
+        pfb::set_error("pfb_sieve_run_noalloc: K = %d is outside [1, %d], the size the fixed scratch holds", K,
+                       PFB_SIEVE_MAX_K);
+        return PFB_E_CAPACITY;
+    }
+    int dev = 0;
+    PFB_CUDA(cudaGetDevice(&dev));
+    NoAllocScratch *sc = nullptr;
+    int sms = 0;
+    int rc = noalloc_scratch(dev, &sc, &sms);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t wpt = pfb_sieve_mask_bytes(K) / 4;
+    if (!(flags & PFB_SIEVE_OR)) PFB_CUDA(cudaMemsetAsync(d_mask, 0, wpt * 4, st));
+    noalloc_begin_kernel<<<1, 1, 0, st>>>(sc, a, b, c);
+    PFB_CUDA(cudaGetLastError());
+    const uint32_t lim = small_limit(K);
+    const uint32_t cap = kNoAllocListCap;
+    if (n_primes) {
+        const int blocks = (int)std::min<uint32_t>((n_primes + 255u) / 256u, (uint32_t)sms * 16u);
+        split_kernel<<<blocks, 256, 0, st>>>(d_primes, n_primes, lim, cap, sc->tiny, sc->small, sc->counts);
+        PFB_CUDA(cudaGetLastError());
+        // record stride 2*cap: tiny then small; the kernels read the counts on the device
+        dim3 g1((2u * cap + 127u) / 128u, 1u);
+        small_setup_kernel<<<g1, 128, 0, st>>>(sc->tiny, sc->small, sc->counts, sc->abc, 1, 2u * cap, sc->rec);
+        PFB_CUDA(cudaGetLastError());
+        const uint32_t tiles = ((uint32_t)K + kTileRows - 1u) / kTileRows;
+        const uint32_t rows = (uint32_t)K < (uint32_t)kTileRows ? (uint32_t)K : (uint32_t)kTileRows;
+        small_tile_kernel<<<dim3(tiles, 1u), kBlockTile, tile_smem_bytes(rows, K), st>>>(sc->rec, sc->counts,
+                                                                                         2u * cap, K, d_mask, wpt);
+        PFB_CUDA(cudaGetLastError());
+        const int lb = (int)((n_primes + kBlockLarge - 1) / kBlockLarge);
+        large_kernel<<<dim3((unsigned)lb, 1u), kBlockLarge, 0, st>>>(d_primes, n_primes, lim, sc->abc, K, d_mask,
+                                                                    wpt);
+        PFB_CUDA(cudaGetLastError());
+    }
+    return PFB_OK;
 }
