@@ -295,6 +295,7 @@ struct pfb_mr {
     int num_sms = 0;
     cudaStream_t stream = nullptr;
     uint32_t *d_tw = nullptr;
+    uint32_t *d_wide = nullptr;
     Twiddles tw{};
 };
 
@@ -345,6 +346,40 @@ static int build_tables(pfb_mr *e) {
         cc.pinv[pr] = 0u - inv;
     }
     PFB_CUDA(cudaMemcpyToSymbol(c_crt, &cc, sizeof(cc)));
+
+    // Wide-pass tables (WideTabs): same twiddles as load_tw, regrouped per j0.
+    WideTabs wt{};
+    std::vector<uint32_t> wide;  // as uint4 planes
+    size_t off4 = 0;
+    for (int dir = 0; dir < 2; dir++)
+        for (int pr = 0; pr < 2; pr++) {
+            const uint32_t *w = h.data() + (size_t)(4 * pr + 2 * dir) * half, *wsh = w + half;
+            for (int lg = LOG_LMIN - 1; lg <= LOG_LMAX; lg++) {
+                const int n = 1 << lg, ng = n >> 4;
+                wt.off[dir][pr][lg] = (uint32_t)off4;
+                wide.resize((off4 + (size_t)8 * ng) * 4, 0u);
+                for (int j0 = 0; j0 < ng; j0++) {
+                    int t = 0;
+                    for (int st = 0; st < 4; st++) {
+                        const int cnt = dir ? (1 << st) : (16 >> (st + 1));
+                        const int lh0 = dir ? lg - 4 : lg - 1;
+                        const int shift = dir ? LOG_LMAX - 1 - (lh0 + st) : LOG_LMAX - 1 - (lh0 - st);
+                        const int step = dir ? ng : ng;  // sub = n/16 (forward), h0 = n/16 (inverse)
+                        for (int e = 0; e < cnt; e++, t++) {
+                            const int k = (j0 + e * step) << shift;
+                            const size_t plane = (size_t)(t >> 2), lane = (size_t)(t & 3);
+                            wide[((off4 + plane * ng + j0) * 4) + lane] = w[k];
+                            wide[((off4 + (4 + plane) * ng + j0) * 4) + lane] = wsh[k];
+                        }
+                    }
+                }
+                off4 += (size_t)8 * ng;
+            }
+        }
+    PFB_CUDA(cudaMalloc(&e->d_wide, wide.size() * sizeof(uint32_t)));
+    PFB_CUDA(cudaMemcpy(e->d_wide, wide.data(), wide.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    wt.base = (const uint4 *)e->d_wide;
+    PFB_CUDA(cudaMemcpyToSymbol(c_wide, &wt, sizeof(wt)));
     return PFB_OK;
 }
 
@@ -392,6 +427,7 @@ extern "C" void pfb_mr_destroy(pfb_mr_t *e) {
         cudaStreamDestroy(e->stream);
     }
     cudaFree(e->d_tw);
+    cudaFree(e->d_wide);
     delete e;
 }
 

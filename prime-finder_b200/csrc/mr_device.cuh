@@ -38,6 +38,37 @@ struct Twiddles {
     const uint32_t *w[2], *wsh[2], *wi[2], *wish[2];
 };
 
+// Twiddles of the one pass per transform in which every group has its own
+// (the first radix-16 pass of a forward transform, the last of an inverse):
+// per (direction, prime, log2 n) eight planes of n/16 uint4, plane q holding
+// twiddles 4q..4q+3 of group j0 at index j0 (planes 0-3 values, 4-7 Shoup
+// companions), so a group reads its 15 + 15 words with 8 coalesced loads.
+struct WideTabs {
+    const uint4 *base;
+    uint32_t off[2][2][LOG_LMAX + 1];  // [forward/inverse][prime][log2 n], in uint4
+};
+__constant__ WideTabs c_wide;
+
+template <int DIR, int PR>
+__device__ __forceinline__ void load_wide(int logn, int j0, uint32_t *tw, uint32_t *tws) {
+    const uint4 *T = c_wide.base + c_wide.off[DIR][PR][logn];
+    const int ng = (1 << logn) >> 4;
+    uint4 v[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) v[q] = __ldg(T + q * ng + j0);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const uint32_t a[4] = {v[q].x, v[q].y, v[q].z, v[q].w};
+        const uint32_t b[4] = {v[4 + q].x, v[4 + q].y, v[4 + q].z, v[4 + q].w};
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            if (4 * q + u < 15) {
+                tw[4 * q + u] = a[u];
+                tws[4 * q + u] = b[u];
+            }
+    }
+}
+
 // Per transform length (index logn): sigma = 2^32 / n mod p (undoes the
 // Montgomery factor of the pointwise product and the 1/n of the inverse).
 struct CrtConsts {
@@ -151,9 +182,11 @@ __device__ __forceinline__ void dif_pass1(uint32_t *__restrict__ A, int logn, in
         }
         return;
     }
+    const bool wide = RLOG == 4 && 2 * h0 == (1 << logn);
     for (int gg = g0; gg < groups; gg += stride) {
         const int block = gg / sub, j0 = gg - block * sub;
-        load_tw<RLOG, false>(W, Wsh, j0, sub, lh0, ta, tsa);
+        if (wide) load_wide<0, PR>(logn, j0, ta, tsa);
+        else load_tw<RLOG, false>(W, Wsh, j0, sub, lh0, ta, tsa);
         dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
     }
 }
@@ -176,9 +209,11 @@ __device__ __forceinline__ void dit_pass1(uint32_t *__restrict__ A, int logn, in
         }
         return;
     }
+    const bool wide = RLOG == 4 && 16 * h0 == (1 << logn);
     for (int gg = g0; gg < groups; gg += stride) {
         const int j0 = gg & (h0 - 1);
-        load_tw<RLOG, true>(W, Wsh, j0, h0, lh0, ta, tsa);
+        if (wide) load_wide<1, PR>(logn, j0, ta, tsa);
+        else load_tw<RLOG, true>(W, Wsh, j0, h0, lh0, ta, tsa);
         dit_group<PR, RLOG>(A, (gg >> lh0) * R * h0 + j0, h0, ta, tsa);
     }
 }
@@ -385,6 +420,42 @@ __device__ __forceinline__ unsigned long long crt(uint32_t r1, uint32_t r2, int 
     return (unsigned long long)c1 + (unsigned long long)P1 * t;
 }
 
+// Pointwise Montgomery product of a transform in shared memory with a stored
+// spectrum in global memory (16-byte loads, 4 consecutive points per thread).
+template <int PR>
+__device__ __forceinline__ void pointwise1(uint32_t *A, const uint32_t *__restrict__ C, int n, const CrtConsts &cc) {
+    constexpr uint32_t p = PR ? P2 : P1;
+    const uint4 *C4 = reinterpret_cast<const uint4 *>(C);
+    for (int i4 = threadIdx.x; i4 < (n >> 2); i4 += blockDim.x) {
+        const uint4 c = __ldg(C4 + i4);
+        const int i = 4 * i4;
+        A[pad(i)] = mont(A[pad(i)], c.x, p, cc.pinv[PR]);
+        A[pad(i + 1)] = mont(A[pad(i + 1)], c.y, p, cc.pinv[PR]);
+        A[pad(i + 2)] = mont(A[pad(i + 2)], c.z, p, cc.pinv[PR]);
+        A[pad(i + 3)] = mont(A[pad(i + 3)], c.w, p, cc.pinv[PR]);
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void pointwise2(uint32_t *A0, uint32_t *A1, const uint32_t *__restrict__ C0,
+                                           const uint32_t *__restrict__ C1, int n, const CrtConsts &cc) {
+    const uint4 *C04 = reinterpret_cast<const uint4 *>(C0);
+    const uint4 *C14 = reinterpret_cast<const uint4 *>(C1);
+    for (int i4 = threadIdx.x; i4 < (n >> 2); i4 += blockDim.x) {
+        const uint4 c = __ldg(C04 + i4), d = __ldg(C14 + i4);
+        const int i = 4 * i4;
+        A0[pad(i)] = mont(A0[pad(i)], c.x, P1, cc.pinv[0]);
+        A0[pad(i + 1)] = mont(A0[pad(i + 1)], c.y, P1, cc.pinv[0]);
+        A0[pad(i + 2)] = mont(A0[pad(i + 2)], c.z, P1, cc.pinv[0]);
+        A0[pad(i + 3)] = mont(A0[pad(i + 3)], c.w, P1, cc.pinv[0]);
+        A1[pad(i)] = mont(A1[pad(i)], d.x, P2, cc.pinv[1]);
+        A1[pad(i + 1)] = mont(A1[pad(i + 1)], d.y, P2, cc.pinv[1]);
+        A1[pad(i + 2)] = mont(A1[pad(i + 2)], d.z, P2, cc.pinv[1]);
+        A1[pad(i + 3)] = mont(A1[pad(i + 3)], d.w, P2, cc.pinv[1]);
+    }
+    __syncthreads();
+}
+
 // Per-CTA view of one candidate.
 struct Cand {
     const uint32_t *nph;   // NTT_L(N')  [2][L] (bit-reversed spectral order)
@@ -445,24 +516,14 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
     }
     // m = T_lo * N' mod R
     dif(A0, A1, logl, tw);
-    for (int i = tid; i < L; i += T) {
-        const int q = pad(i);
-        A0[q] = mont(A0[q], __ldg(cd.nph + i), P1, cc.pinv[0]);
-        A1[q] = mont(A1[q], __ldg(cd.nph + L + i), P2, cc.pinv[1]);
-    }
-    __syncthreads();
+    pointwise2(A0, A1, cd.nph, cd.nph + L, L, cc);
     dit(A0, A1, logl, tw);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
     for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1): cyclic product of length H
     dif(A0, A1, logl - 1, tw);
-    for (int i = tid; i < H; i += T) {
-        const int q = pad(i);
-        A0[q] = mont(A0[q], __ldg(cd.nh + i), P1, cc.pinv[0]);
-        A1[q] = mont(A1[q], __ldg(cd.nh + H + i), P2, cc.pinv[1]);
-    }
-    __syncthreads();
+    pointwise2(A0, A1, cd.nh, cd.nh + H, H, cc);
     dit(A0, A1, logl - 1, tw);
     const unsigned long long cW =
         carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl - 1, cc); }, A0, cs);
@@ -533,29 +594,25 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     }
     // m = T_lo * N' mod R
     dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
-    for (int i = tid; i < L; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nph + i), P1, cc.pinv[0]);
-    __syncthreads();
+    pointwise1<0>(A, cd.nph, L, cc);
     dit1<0>(A, logl, tw.wi[0], tw.wish[0]);
     spill(H);
     load_x(sp.t, true);
     dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
-    for (int i = tid; i < L; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nph + L + i), P2, cc.pinv[1]);
-    __syncthreads();
+    pointwise1<1>(A, cd.nph + L, L, cc);
     dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
     for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1)
     dif1<0>(A, logl - 1, tw.w[0], tw.wsh[0]);
-    for (int i = tid; i < H; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nh + i), P1, cc.pinv[0]);
-    __syncthreads();
+    pointwise1<0>(A, cd.nh, H, cc);
     dit1<0>(A, logl - 1, tw.wi[0], tw.wish[0]);
     spill(H);
     for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
     __syncthreads();
     dif1<1>(A, logl - 1, tw.w[1], tw.wsh[1]);
-    for (int i = tid; i < H; i += T) A[pad(i)] = mont(A[pad(i)], __ldg(cd.nh + H + i), P2, cc.pinv[1]);
-    __syncthreads();
+    pointwise1<1>(A, cd.nh + H, H, cc);
     dit1<1>(A, logl - 1, tw.wi[1], tw.wish[1]);
     const unsigned long long cW = carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl - 1, cc); }, A, cs);

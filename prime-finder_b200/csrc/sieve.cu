@@ -328,40 +328,44 @@ large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
         for (int lk = 1; lk <= maxd; lk++) {  // rev form, per digit class of k
             if (!(lc.flags & (1u << lk))) continue;
             const uint32_t lo = pow10i(lk - 1), hi = pow10i(lk) - 1u;
-            uint32_t jl[4], step[4];
-            int nj = 0;
-            uint32_t tv[4];
-            for (int lj = 1; lj <= maxd; lj++) {
-                if (!(lc.flags & (1u << (4 + lj)))) continue;
-                jl[nj] = (uint32_t)lj;
-                step[nj] = lc.br[lk - 1][lj - 1];
-                tv[nj] = lc.ar[lj - 1];
-                nj++;
+            // State of the four j classes in registers.  A class that is off
+            // (no such digit count on the grid, or skipped by the reference's
+            // rules) keeps value 0 and step 0: 0 never passes the hit test.
+            uint32_t tv[4], st[4], on = 0u;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const bool c_on = (q + 1 <= maxd) && (lc.flags & (1u << (5 + q)));
+                on |= c_on ? (1u << q) : 0u;
+                st[q] = c_on ? lc.br[lk - 1][q] : 0u;
+                tv[q] = c_on ? lc.ar[q] : 0u;
             }
             if (hi <= (uint32_t)K) {
                 // every lk-digit k is on the grid: walk rev(k) = 1 .. hi linearly
-                for (int q = 0; q < nj; q++) tv[q] = M.sub(tv[q], step[q]);  // rk = 1
+#pragma unroll
+                for (int q = 0; q < 4; q++) tv[q] = M.sub(tv[q], st[q]);  // rk = 1
                 for (uint32_t rk = 1; rk <= hi; rk++) {
-                    for (int q = 0; q < nj; q++) {
-                        const uint32_t lim = pow10i(jl[q]);
-                        if (tv[q] - 1u < lim - 1u) {  // 1 <= rev(j) < 10^lj
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (tv[q] - 1u < pow10i(q + 1) - 1u) {  // 1 <= rev(j) < 10^(q+1)
                             const uint32_t rj = tv[q];
-                            if ((lk == 1 || rk % 10u != 0u) && (jl[q] == 1 || rj % 10u != 0u)) {
-                                const uint32_t j = rev_digits(rj, jl[q]);
+                            if ((lk == 1 || rk % 10u != 0u) && (q == 0 || rj % 10u != 0u)) {
+                                const uint32_t j = rev_digits(rj, q + 1);
                                 if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
                             }
                         }
-                        tv[q] = M.sub(tv[q], step[q]);
+                        tv[q] = M.sub(tv[q], st[q]);
                     }
                 }
             } else {
                 // partial top class (K < 10^lk - 1): visit the k on the grid directly
                 for (uint32_t k = lo; k <= (uint32_t)K; k++) {
                     const uint32_t rk = rev_digits(k, lk) % p;
-                    for (int q = 0; q < nj; q++) {
-                        const uint32_t rj = M.sub(lc.ar[jl[q] - 1], M.mul(rk, step[q]));
-                        if (rj - 1u < pow10i(jl[q]) - 1u && (jl[q] == 1 || rj % 10u != 0u)) {
-                            const uint32_t j = rev_digits(rj, jl[q]);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        if (!(on & (1u << q))) continue;
+                        const uint32_t rj = M.sub(lc.ar[q], M.mul(rk, st[q]));
+                        if (rj - 1u < pow10i(q + 1) - 1u && (q == 0 || rj % 10u != 0u)) {
+                            const uint32_t j = rev_digits(rj, q + 1);
                             if (j <= (uint32_t)K) mark_global(m, K, k, j);
                         }
                     }
