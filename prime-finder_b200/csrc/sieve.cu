@@ -17,8 +17,10 @@
 //    spread over 32 lanes.  The finished tile is OR-ed into global memory
 //    with coalesced 32-bit atomics.
 //  * Large primes (p >= S) hit each row at most once.  One thread per prime
-//    walks the lines with incremental modular updates (no multiplications in
-//    the loop) and OR-s the rare hits into global memory.
+//    enumerates the hits of its long lines with a lattice walk (O(log p) per
+//    line plus O(1) per hit), iterates the short lines (<= 99 values on one
+//    side) with incremental modular updates, and OR-s the hits into global
+//    memory.
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdint.h>
@@ -179,6 +181,124 @@ __device__ __forceinline__ void mark_global(uint32_t *mask, int K, uint32_t k, u
 }
 
 // ---------------------------------------------------------------------------
+// Lattice enumeration of one line.  The hits of y == A - B x (mod p) with x in
+// [x0, x1] and 1 <= y <= Y (Y < p) are the points of a translate of the
+// lattice {(i, t) : i == g t (mod p)}, g = -B, that fall in the strip
+// 0 <= i < Y (i = y - 1, t = x - x0).
+//
+//  * first_hit: the smallest t >= 0 with (c + g t) mod p < Y, by a Euclid-like
+//    descent on (multiplier, modulus) that halves the modulus every level
+//    (reflection keeps the multiplier below half the modulus): depth <= 33.
+//  * fk_reduce: a basis u = (-a, beta), v = (c, delta) with 0 <= a, c < Y,
+//    a + c >= Y, beta, delta > 0 (Franke and Kleinjung, "Continued fractions
+//    and lattice sieving", 2005).  From a strip point (i, t) the next strip
+//    point is (i, t) + u if i >= a, + v if i + c < Y, else + u + v.
+// Cost: O(log p) per line plus O(1) per hit, where walking the K values of x
+// costs O(K).
+
+__device__ __forceinline__ uint32_t ceil_div64(unsigned long long n, uint32_t d) {
+    return (uint32_t)((n + d - 1ull) / d);
+}
+
+__device__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, uint32_t Y) {
+    if (c < Y) return 0u;
+    uint32_t a = g, m = p, L = p - c, R = p - c + Y - 1u;
+    uint32_t sm[34], sa[34], sl[34];
+    int d = 0;
+    uint32_t x;
+    for (;;) {
+        const uint32_t k = (L - 1u) / a + 1u;  // ceil(L / a), L >= 1
+        if ((unsigned long long)a * k <= R) {
+            x = k;
+            break;
+        }
+        if (d >= 34) return 0xFFFFFFFFu;  // unreachable: the modulus halves each level
+        sm[d] = m;
+        sa[d] = a;
+        sl[d] = L;
+        d++;
+        const uint32_t r = m % a;           // != 0: gcd(a, m) = 1 along the chain
+        uint32_t a2 = a - r, L2 = L % a, R2 = R % a;
+        const uint32_t m2 = a;
+        if (a2 > (m2 >> 1)) {               // reflect: a x in [L, R] <=> (m - a) x in [m - R, m - L]
+            a2 = r;
+            const uint32_t t2 = m2 - R2;
+            R2 = m2 - L2;
+            L2 = t2;
+        }
+        a = a2;
+        m = m2;
+        L = L2;
+        R = R2;
+    }
+    while (d > 0) {
+        d--;
+        x = ceil_div64((unsigned long long)x * sm[d] + sl[d], sa[d]);
+    }
+    return x;
+}
+
+struct FKBasis {
+    uint32_t a, beta, c, delta;
+};
+
+__device__ FKBasis fk_reduce(uint32_t g, uint32_t p, uint32_t I) {
+    uint32_t a = p, beta = 0u, c = g, delta = 1u;
+    for (;;) {
+        if (c < I) {
+            const uint32_t k = (a - (I - c)) / c;
+            a -= k * c;
+            beta += k * delta;
+            break;
+        }
+        if (a < I) {
+            const uint32_t k = (c - (I - a)) / a;
+            c -= k * a;
+            delta += k * beta;
+            break;
+        }
+        if (a >= c) {
+            const uint32_t k = a / c;
+            a -= k * c;
+            beta += k * delta;
+        } else {
+            const uint32_t k = c / a;
+            c -= k * a;
+            delta += k * beta;
+        }
+    }
+    return FKBasis{a, beta, c, delta};
+}
+
+// Calls visit(x, y) for every x in [x0, x1] with y = (A - B x) mod p in
+// [1, Y]; requires 1 <= Y < p, B != 0 (mod p), x1 - x0 < p.
+template <class Visit>
+__device__ __forceinline__ void line_hits(const Mod32 &M, uint32_t A, uint32_t B, uint32_t x0, uint32_t x1,
+                                          uint32_t Y, Visit visit) {
+    const uint32_t p = M.p;
+    const uint32_t g = p - B;
+    const uint32_t c0 = M.sub(M.sub(A, 1u % p), M.mul(B, x0 % p));  // (A - 1 - B x0) mod p
+    unsigned long long t = first_hit(c0, g, p, Y);
+    const unsigned long long span = (unsigned long long)(x1 - x0);
+    if (t > span) return;
+    const FKBasis fb = fk_reduce(g, p, Y);
+    uint32_t i = M.red((unsigned long long)g * t + c0);
+    while (t <= span) {
+        visit(x0 + (uint32_t)t, i + 1u);
+        if (i >= fb.a) {
+            i -= fb.a;
+            t += fb.beta;
+        } else if (i + fb.c < Y) {
+            i += fb.c;
+            t += fb.delta;
+        } else {
+            i = i - fb.a + fb.c;
+            t += (unsigned long long)fb.beta + fb.delta;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Prime-list split: tiny (p < 512), small (512 <= p < S); large primes are
 // filtered inside the large-prime kernel.
 // A list with repeated entries can exceed `cap`; the excess is counted but
@@ -318,13 +438,9 @@ large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
         LineConsts lc;
         line_consts(M, a, b, c, lc);
 
-        if (lc.flags & 1u) {  // N form
-            uint32_t j = M.sub(lc.an, lc.bn);  // k = 1
-            for (uint32_t k = 1; k <= (uint32_t)K; k++) {
-                if (j - 1u < (uint32_t)K) mark_global(m, K, k, j);
-                j = M.sub(j, lc.bn);
-            }
-        }
+        if (lc.flags & 1u)  // N form: j == AN - k BN (p > K: at most one j per k)
+            line_hits(M, lc.an, lc.bn, 1u, (uint32_t)K, (uint32_t)K,
+                      [&](uint32_t k, uint32_t j) { mark_global(m, K, k, j); });
         for (int lk = 1; lk <= maxd; lk++) {  // rev form, per digit class of k
             if (!(lc.flags & (1u << lk))) continue;
             const uint32_t lo = pow10i(lk - 1), hi = pow10i(lk) - 1u;
@@ -339,8 +455,37 @@ large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
                 st[q] = c_on ? lc.br[lk - 1][q] : 0u;
                 tv[q] = c_on ? lc.ar[q] : 0u;
             }
-            if (hi <= (uint32_t)K) {
-                // every lk-digit k is on the grid: walk rev(k) = 1 .. hi linearly
+            if (hi <= (uint32_t)K && lk >= 3) {
+                // Long class (rev(k) takes up to 9999 values): per j class, a
+                // lattice walk when rev(j) has >= 3 digits; otherwise iterate
+                // the <= 99 values of rev(j): rev(k) == (AR - rev(j)) BR^-1,
+                // BR^-1 = 10^(b-c+lk-lj) = BN * 10^(lk-lj).
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    if (!(on & (1u << q))) continue;
+                    const int lj = q + 1;
+                    const uint32_t ylim = pow10i(lj) - 1u;
+                    if (lj >= 3) {
+                        line_hits(M, lc.ar[q], st[q], 1u, hi, ylim, [&](uint32_t rk, uint32_t rj) {
+                            if (rk % 10u != 0u && rj % 10u != 0u) {
+                                const uint32_t j = rev_digits(rj, lj);
+                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
+                            }
+                        });
+                    } else {
+                        const uint32_t inv = M.mul(lc.bn, pow10i(lk - lj) % p);
+                        uint32_t rk = M.mul(lc.ar[q], inv);  // rev(j) = 0
+                        for (uint32_t rj = 1; rj <= ylim; rj++) {
+                            rk = M.sub(rk, inv);
+                            if (rk - 1u < hi && rk % 10u != 0u && (lj == 1 || rj % 10u != 0u)) {
+                                const uint32_t j = rev_digits(rj, lj);
+                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
+                            }
+                        }
+                    }
+                }
+            } else if (hi <= (uint32_t)K) {
+                // short class (lk <= 2): walk rev(k) = 1 .. hi linearly
 #pragma unroll
                 for (int q = 0; q < 4; q++) tv[q] = M.sub(tv[q], st[q]);  // rk = 1
                 for (uint32_t rk = 1; rk <= hi; rk++) {
