@@ -347,24 +347,27 @@ static int build_tables(pfb_mr *e) {
     }
     PFB_CUDA(cudaMemcpyToSymbol(c_crt, &cc, sizeof(cc)));
 
-    // Wide-pass tables (WideTabs): same twiddles as load_tw, regrouped per j0.
+    // Radix-16 pass tables (WideTabs): the twiddles load_tw would read, regrouped
+    // per j0, for every first-stage half size h0 a pass can have.
     WideTabs wt{};
     std::vector<uint32_t> wide;  // as uint4 planes
     size_t off4 = 0;
     for (int dir = 0; dir < 2; dir++)
         for (int pr = 0; pr < 2; pr++) {
             const uint32_t *w = h.data() + (size_t)(4 * pr + 2 * dir) * half, *wsh = w + half;
-            for (int lg = LOG_LMIN - 1; lg <= LOG_LMAX; lg++) {
-                const int n = 1 << lg, ng = n >> 4;
-                wt.off[dir][pr][lg] = (uint32_t)off4;
+            // forward passes: h0 = 8 .. 2^(LOG_LMAX-1), groups j0 < h0/8, element step h0/8;
+            // inverse passes: h0 = 1 .. 2^(LOG_LMAX-4), groups j0 < h0, element step h0
+            const int lmin = dir ? 0 : 3, lmax = dir ? LOG_LMAX - 4 : LOG_LMAX - 1;
+            for (int lh0 = lmin; lh0 <= lmax; lh0++) {
+                const int ng = dir ? (1 << lh0) : (1 << (lh0 - 3));
+                const int step = ng;
+                wt.off[dir][pr][lh0] = (uint32_t)off4;
                 wide.resize((off4 + (size_t)8 * ng) * 4, 0u);
                 for (int j0 = 0; j0 < ng; j0++) {
                     int t = 0;
                     for (int st = 0; st < 4; st++) {
                         const int cnt = dir ? (1 << st) : (16 >> (st + 1));
-                        const int lh0 = dir ? lg - 4 : lg - 1;
                         const int shift = dir ? LOG_LMAX - 1 - (lh0 + st) : LOG_LMAX - 1 - (lh0 - st);
-                        const int step = dir ? ng : ng;  // sub = n/16 (forward), h0 = n/16 (inverse)
                         for (int e = 0; e < cnt; e++, t++) {
                             const int k = (j0 + e * step) << shift;
                             const size_t plane = (size_t)(t >> 2), lane = (size_t)(t & 3);

@@ -38,21 +38,22 @@ struct Twiddles {
     const uint32_t *w[2], *wsh[2], *wi[2], *wish[2];
 };
 
-// Twiddles of the one pass per transform in which every group has its own
-// (the first radix-16 pass of a forward transform, the last of an inverse):
-// per (direction, prime, log2 n) eight planes of n/16 uint4, plane q holding
-// twiddles 4q..4q+3 of group j0 at index j0 (planes 0-3 values, 4-7 Shoup
-// companions), so a group reads its 15 + 15 words with 8 coalesced loads.
+// Twiddles of every radix-16 pass, regrouped per group: a pass's twiddles
+// depend only on its first stage's half size h0 and the group's j0, so per
+// (direction, prime, log2 h0) there are eight planes of G uint4 (G = h0/8
+// groups for a forward pass, h0 for an inverse one); plane q holds twiddles
+// 4q..4q+3 of group j0 at index j0 (planes 0-3 values, 4-7 Shoup
+// companions).  A group reads its 15 + 15 words with 8 coalesced loads.
 struct WideTabs {
     const uint4 *base;
-    uint32_t off[2][2][LOG_LMAX + 1];  // [forward/inverse][prime][log2 n], in uint4
+    uint32_t off[2][2][LOG_LMAX];  // [forward/inverse][prime][log2 h0], in uint4
 };
 __constant__ WideTabs c_wide;
 
 template <int DIR, int PR>
-__device__ __forceinline__ void load_wide(int logn, int j0, uint32_t *tw, uint32_t *tws) {
-    const uint4 *T = c_wide.base + c_wide.off[DIR][PR][logn];
-    const int ng = (1 << logn) >> 4;
+__device__ __forceinline__ void load_wide(int lh0, int j0, uint32_t *tw, uint32_t *tws) {
+    const uint4 *T = c_wide.base + c_wide.off[DIR][PR][lh0];
+    const int ng = DIR ? (1 << lh0) : (1 << (lh0 - 3));
     uint4 v[8];
 #pragma unroll
     for (int q = 0; q < 8; q++) v[q] = __ldg(T + q * ng + j0);
@@ -175,17 +176,17 @@ __device__ __forceinline__ void dif_pass1(uint32_t *__restrict__ A, int logn, in
     const int lh0 = 31 - __clz(h0);
     uint32_t ta[R - 1], tsa[R - 1];
     if (stride % sub == 0) {
-        load_tw<RLOG, false>(W, Wsh, g0 % sub, sub, lh0, ta, tsa);
+        if (RLOG == 4) load_wide<0, PR>(lh0, g0 % sub, ta, tsa);
+        else load_tw<RLOG, false>(W, Wsh, g0 % sub, sub, lh0, ta, tsa);
         for (int gg = g0; gg < groups; gg += stride) {
             const int block = gg / sub, j0 = gg - block * sub;
             dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
         }
         return;
     }
-    const bool wide = RLOG == 4 && 2 * h0 == (1 << logn);
     for (int gg = g0; gg < groups; gg += stride) {
         const int block = gg / sub, j0 = gg - block * sub;
-        if (wide) load_wide<0, PR>(logn, j0, ta, tsa);
+        if (RLOG == 4) load_wide<0, PR>(lh0, j0, ta, tsa);
         else load_tw<RLOG, false>(W, Wsh, j0, sub, lh0, ta, tsa);
         dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
     }
@@ -202,17 +203,17 @@ __device__ __forceinline__ void dit_pass1(uint32_t *__restrict__ A, int logn, in
     const int lh0 = 31 - __clz(h0);
     uint32_t ta[R - 1], tsa[R - 1];
     if (stride % h0 == 0) {
-        load_tw<RLOG, true>(W, Wsh, g0 & (h0 - 1), h0, lh0, ta, tsa);
+        if (RLOG == 4) load_wide<1, PR>(lh0, g0 & (h0 - 1), ta, tsa);
+        else load_tw<RLOG, true>(W, Wsh, g0 & (h0 - 1), h0, lh0, ta, tsa);
         for (int gg = g0; gg < groups; gg += stride) {
             const int block = gg >> lh0, j0 = gg & (h0 - 1);
             dit_group<PR, RLOG>(A, block * R * h0 + j0, h0, ta, tsa);
         }
         return;
     }
-    const bool wide = RLOG == 4 && 16 * h0 == (1 << logn);
     for (int gg = g0; gg < groups; gg += stride) {
         const int j0 = gg & (h0 - 1);
-        if (wide) load_wide<1, PR>(logn, j0, ta, tsa);
+        if (RLOG == 4) load_wide<1, PR>(lh0, j0, ta, tsa);
         else load_tw<RLOG, true>(W, Wsh, j0, h0, lh0, ta, tsa);
         dit_group<PR, RLOG>(A, (gg >> lh0) * R * h0 + j0, h0, ta, tsa);
     }

@@ -200,7 +200,7 @@ __device__ __forceinline__ uint32_t ceil_div64(unsigned long long n, uint32_t d)
     return (uint32_t)((n + d - 1ull) / d);
 }
 
-__device__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, uint32_t Y) {
+__device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, uint32_t Y) {
     if (c < Y) return 0u;
     uint32_t a = g, m = p, L = p - c, R = p - c + Y - 1u;
     uint32_t sm[34], sa[34], sl[34];
@@ -242,7 +242,7 @@ struct FKBasis {
     uint32_t a, beta, c, delta;
 };
 
-__device__ FKBasis fk_reduce(uint32_t g, uint32_t p, uint32_t I) {
+__device__ __noinline__ FKBasis fk_reduce(uint32_t g, uint32_t p, uint32_t I) {
     uint32_t a = p, beta = 0u, c = g, delta = 1u;
     for (;;) {
         if (c < I) {
@@ -459,8 +459,9 @@ large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
                 // Long class (rev(k) takes up to 9999 values): per j class, a
                 // lattice walk when rev(j) has >= 3 digits; otherwise iterate
                 // the <= 99 values of rev(j): rev(k) == (AR - rev(j)) BR^-1,
-                // BR^-1 = 10^(b-c+lk-lj) = BN * 10^(lk-lj).
-#pragma unroll
+                // BR^-1 = 10^(b-c+lk-lj) = BN * 10^(lk-lj).  (Not unrolled:
+                // the walk is large and the instruction cache small.)
+#pragma unroll 1
                 for (int q = 0; q < 4; q++) {
                     if (!(on & (1u << q))) continue;
                     const int lj = q + 1;
