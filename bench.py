@@ -224,6 +224,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--sieve-triples", type=int, default=4)
+    ap.add_argument("--serve-secs", type=float, default=0.0,
+                    help="also run the serving loop (Poisson arrivals, config 5 shapes) this long")
+    ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -348,6 +351,7 @@ def main():
         stream.synchronize()
         barrier()
         times = []
+        done0 = pfb200.batch_steps_done(batch)
         with ClockSampler(dev) as clocks:
             for _ in range(args.steps):
                 flush.fill_(1)  # L2 flush between timed steps (outside the events)
@@ -357,10 +361,11 @@ def main():
                 e1.record(stream)
                 stream.synchronize()
                 times.append(e0.elapsed_time(e1) / 1e3)
+        done1 = pfb200.batch_steps_done(batch)
         barrier()
     t_mr = max_over_ranks(sum(times))
     n = len(cands)
-    squarings = n * chunk * args.steps
+    squarings = done1 - done0  # steps the device executed in the timed launches
     tests_s = squarings / sq_per_test / t_mr * world
     ms_per_step = 1e3 * t_mr / args.steps
     batch.close()
@@ -370,12 +375,14 @@ def main():
     with torch.cuda.stream(stream):
         one.advance(256, stream.cuda_stream)
         stream.synchronize()
+        d0 = pfb200.batch_steps_done(one)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         one.advance(1024, stream.cuda_stream)
         e1.record(stream)
         stream.synchronize()
-    plain_sq_s = 1024 / (e0.elapsed_time(e1) / 1e3)
+        d1 = pfb200.batch_steps_done(one)
+    plain_sq_s = (d1 - d0) / (e0.elapsed_time(e1) / 1e3)
     plain_tests_s = plain_sq_s / sq_per_test
     one.close()
 
@@ -389,6 +396,46 @@ def main():
                 "peak_source": "measured live: pfb_measure_int32_peak (mul.lo)",
                 "mul_hi_peak": peak_hi / 1e12,
                 "work": "%d INT32 multiplies per squaring (reference structure at %d digits)" % (ref_mults, digits)}
+
+    # --- serving: continuous batching under Poisson arrivals ---------------
+    serving = None
+    if args.serve_secs > 0:
+        import random
+        rng = random.Random(3)
+        # requests: N and rev(N) as separate requests, a ~ U[50000, 100000], c ~ U[100, 1000],
+        # b ~ U[c+1, a-1] (redrawn while a-b-lk < 2 or b-c <= lj), k, j ~ U[1, 9999]
+        def draw():
+            while True:
+                a = rng.randint(50000, 100000)
+                c = rng.randint(100, 1000)
+                b = rng.randint(c + 1, a - 1)
+                k, j = rng.randint(1, 9999), rng.randint(1, 9999)
+                if a - b - len(str(k)) >= 2 and b - c > len(str(j)):
+                    return pfb200.build_candidate(a, b, c, k, j, bool(rng.getrandbits(1)))
+        props = torch.cuda.get_device_properties(dev)
+        cap_tests_s = squarings / t_mr / (2.25 * sq_per_test * 2.5)  # mean size ~75k digits: ~2.25x bits, ~2.5x time/step
+        rate = args.serve_load * cap_tests_s
+        srv = pfb200.MRServer(eng, max_resident=2 * props.multi_processor_count, chunk_steps=256)
+        t_start = time.perf_counter()
+        next_t, tag, lat, pending = 0.0, 0, [], 0
+        while time.perf_counter() - t_start < args.serve_secs:
+            now = time.perf_counter() - t_start
+            while next_t <= now:
+                srv.submit(draw(), tag)
+                tag += 1
+                next_t += rng.expovariate(rate)
+            for r in srv.poll(256, 50):
+                lat.append(r["done_s"] - r["submit_s"])
+        st = srv.stats()
+        srv.close()
+        lat.sort()
+        pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
+        serving = {"seconds": args.serve_secs, "arrival_rate_per_s": rate, "submitted": tag,
+                   "completed": len(lat), "tests_per_s": len(lat) / args.serve_secs,
+                   "p50_s": pct(0.50), "p99_s": pct(0.99), "resident_at_end": st["resident"],
+                   "queued_at_end": st["queued"], "launches": st["launches"],
+                   "workload": "Poisson arrivals (seed 3) of N / rev(N), a ~ U[50000,100000], "
+                               "k,j ~ U[1,9999], at %.2fx the estimated capacity" % args.serve_load}
 
     # --- e2e through the C ABI ---------------------------------------------
     e2e = None
@@ -430,6 +477,7 @@ def main():
         "roofline": roofline,
         "cpu_baseline": cpu,
         "cpu_baseline_sieve": cpu_sieve,
+        "serving": serving,
         "clocks": clocks.summary(),
         "e2e": e2e,
         "gpu_launches": args.steps * launches_per_step,

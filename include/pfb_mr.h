@@ -71,7 +71,10 @@ int pfb_mr_powm(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,
  * memory between calls).  A step is one modular squaring of every unfinished
  * candidate (or one verdict check).
  *   create   host set-up, upload and transforms of N and N' (synchronous)
- *   advance  enqueue `steps` steps on `stream` (NULL = engine stream)
+ *   advance  enqueue about `steps` steps of every unfinished candidate on
+ *            `stream` (NULL = engine stream): a persistent kernel, one CTA
+ *            per SM, hands out quanta of 64 steps round-robin, so the SMs
+ *            stay busy whatever the number and lengths of the candidates
  *   pending  number of unfinished candidates (synchronises the device)
  *   results  verdicts / residues as in pfb_mr_test; PFB_E_STATE while some
  *            candidate is unfinished (its verdict is reported as -2)
@@ -81,9 +84,55 @@ int pfb_mr_batch_create(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_
                         pfb_mr_batch_t **out);
 int pfb_mr_batch_advance(pfb_mr_batch_t *b, int steps, void *stream);
 int pfb_mr_batch_pending(pfb_mr_batch_t *b, int *pending);
+/* Steps (squarings + checks) executed so far over all candidates (synchronises). */
+long long pfb_mr_batch_steps_done(pfb_mr_batch_t *b);
 long long pfb_mr_batch_steps_left(pfb_mr_batch_t *b);
 int pfb_mr_batch_results(pfb_mr_batch_t *b, int8_t *verdict, uint16_t *residue, int residue_stride);
 void pfb_mr_batch_destroy(pfb_mr_batch_t *b);
+
+/*
+ * Serving: continuous batching of strong tests (no counterpart in the
+ * reference, which tests one fixed batch per call: bench_mr_gpu.cu:209-256).
+ * Requests arrive one by one from any thread; host workers do the set-up;
+ * a driver thread admits prepared requests into free device slots as slots
+ * and the HBM budget allow, advances every resident candidate by
+ * chunk_steps per launch of the persistent kernel (candidates of different
+ * lengths share every launch), and retires finished ones.  Per-candidate
+ * residue and exponent cursor live in device memory for the whole test.
+ */
+typedef struct pfb_mr_server pfb_mr_server_t;
+
+typedef struct {
+    int max_resident;          /* candidates on the GPU at once (0: 2 per SM)      */
+    size_t hbm_budget_bytes;   /* cap on slot memory owned (0: no cap)             */
+    int chunk_steps;           /* steps per candidate per launch (0: 512)          */
+    uint32_t base;             /* witness, 2 <= base < 65536 (0: 2)                */
+    int prep_threads;          /* host set-up threads (0: 4)                       */
+} pfb_mr_server_config_t;
+
+typedef struct {
+    uint64_t tag;              /* caller's tag from pfb_mr_server_submit           */
+    int8_t verdict;            /* 1 probable prime, 0 composite, -1 invalid input  */
+    double submit_s, admit_s, done_s;  /* seconds since the server started         */
+} pfb_mr_result_t;
+
+typedef struct {
+    long long submitted, admitted, completed, launches, steps_retired;
+    int resident, queued, error;
+    size_t bytes_in_use, bytes_owned;
+} pfb_mr_server_stats_t;
+
+int pfb_mr_server_create(pfb_mr_t *e, const pfb_mr_server_config_t *cfg, pfb_mr_server_t **out);
+/* Queue N (16-bit limbs, copied).  residue_out (optional, host, residue_cap
+ * limbs) receives base^d mod N before the result is posted. */
+int pfb_mr_server_submit(pfb_mr_server_t *s, const uint16_t *limbs, int n_limbs, uint64_t tag,
+                         uint16_t *residue_out, int residue_cap);
+/* Up to cap finished results, waiting at most timeout_ms; returns their
+ * number, or a negative PFB_E* code if the server stopped on an error. */
+int pfb_mr_server_poll(pfb_mr_server_t *s, pfb_mr_result_t *out, int cap, int timeout_ms);
+int pfb_mr_server_stats(pfb_mr_server_t *s, pfb_mr_server_stats_t *st);
+/* Stops the loop (pending requests are dropped) and frees everything. */
+void pfb_mr_server_destroy(pfb_mr_server_t *s);
 
 /* Squarings (plus the final conversion) a strong test of N costs: the unit of
  * the engine's throughput counters. */

@@ -71,9 +71,9 @@ __device__ __forceinline__ void carve(uint32_t *raw, int logl, Smem &sm, uint32_
     sm.cs = (CarrySmem *)c;
 }
 
-__global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, Twiddles tw) {
+__global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, const int *list, Twiddles tw) {
     extern __shared__ __align__(16) uint32_t raw[];
-    const JobDev jb = jobs[blockIdx.x];
+    const JobDev jb = jobs[list ? list[blockIdx.x] : (int)blockIdx.x];
     if (jb.phase == 3) return;
     Smem sm;
     uint32_t *Y;
@@ -151,17 +151,24 @@ __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uin
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(THREADS, 1) step_kernel(JobDev *jobs, int max_steps, Twiddles tw) {
-    extern __shared__ __align__(16) uint32_t raw[];
-    JobDev *jp = jobs + blockIdx.x;
-    const JobDev jb = *jp;
+// Runs up to max_steps steps of one candidate.  The job's state is read with
+// L2 loads (__ldcg): in the persistent kernel another SM may have written it
+// earlier in the same launch.
+__device__ void run_job(JobDev *jp, int max_steps, const Twiddles &tw, uint32_t *raw) {
+    JobDev jb;
+    {
+        const unsigned long long *src = reinterpret_cast<const unsigned long long *>(jp);
+        unsigned long long *dst = reinterpret_cast<unsigned long long *>(&jb);
+#pragma unroll
+        for (int w = 0; w < (int)(sizeof(JobDev) / 8); w++) dst[w] = __ldcg(src + w);
+    }
     if (jb.phase == 3) return;
     Smem sm;
     uint32_t *Y;
     carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int H = 1 << (jb.logl - 1);
     const Cand cd{jb.nph, jb.nh, jb.logl};
-    for (int i = threadIdx.x; i < H; i += blockDim.x) sm.X[i] = jb.x[i];
+    for (int i = threadIdx.x; i < H; i += blockDim.x) sm.X[i] = __ldcg(jb.x + i);
     __syncthreads();
 
     int cursor = jb.cursor, phase = jb.phase, extra = jb.extra, verdict = jb.verdict, steps = 0;
@@ -209,6 +216,48 @@ __global__ void __launch_bounds__(THREADS, 1) step_kernel(JobDev *jobs, int max_
         jp->extra = extra;
         jp->verdict = verdict;
         jp->steps = jb.steps + steps;
+    }
+    __syncthreads();
+}
+
+// Persistent scheduler: one CTA per SM takes quanta (`quantum` steps of one
+// candidate) until `total` quanta are handed out.  Quantum q goes to the
+// first unfinished, unlocked candidate at or after q mod n, so candidates
+// advance round-robin and no SM idles while work remains.  Nothing waits: a
+// CTA that finds every candidate locked or finished leaves.
+__global__ void __launch_bounds__(THREADS, 1)
+persist_kernel(JobDev *jobs, int n, int *locks, unsigned int *counter, unsigned int total, int quantum,
+               Twiddles tw) {
+    extern __shared__ __align__(16) uint32_t raw[];
+    __shared__ int s_job;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            int job = -1;
+            const unsigned int q = atomicAdd(counter, 1u);
+            if (q < total) {
+                for (int probe = 0; probe < n; probe++) {
+                    const int j = (int)((q + (unsigned int)probe) % (unsigned int)n);
+                    if (__ldcg(&jobs[j].phase) == 3) continue;
+                    if (atomicCAS(&locks[j], 0, 1) != 0) continue;
+                    __threadfence();
+                    if (__ldcg(&jobs[j].phase) != 3) {
+                        job = j;
+                        break;
+                    }
+                    atomicExch(&locks[j], 0);
+                }
+            }
+            s_job = job;
+        }
+        __syncthreads();
+        const int j = s_job;
+        __syncthreads();
+        if (j < 0) break;
+        run_job(jobs + j, quantum, tw, raw);
+        if (threadIdx.x == 0) {
+            __threadfence();
+            atomicExch(&locks[j], 0);
+        }
     }
 }
 
@@ -408,7 +457,7 @@ extern "C" int pfb_mr_create(pfb_mr_t **out, int device) {
     if (!rc) rc = build_tables(e);
     if (!rc) {
         const int mx = (int)std::max(smem_bytes(LOG_LCTA), smem_bytes(LOG_LSEQ));
-        ce = cudaFuncSetAttribute(step_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        ce = cudaFuncSetAttribute(persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         if (ce == cudaSuccess) ce = cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "smem attribute", __FILE__, __LINE__);
     }
@@ -441,8 +490,8 @@ struct Layout {
     size_t x, res, nph, nh, npl, nl, exp, ss, st, yb, total;
 };
 
-Layout layout_for(const HostPrep &hp) {
-    const size_t L = (size_t)1 << hp.logl, H = L / 2;
+Layout layout_for(int logl, size_t exp_words) {
+    const size_t L = (size_t)1 << logl, H = L / 2;
     Layout l{};
     size_t o = 0;
     auto take = [&](size_t words) {
@@ -456,14 +505,23 @@ Layout layout_for(const HostPrep &hp) {
     l.nh = take(2 * H);
     l.npl = take(H);
     l.nl = take(H);
-    l.exp = take(hp.exp.size());
-    if (hp.logl > LOG_LCTA) {
+    l.exp = take(exp_words);
+    if (logl > LOG_LCTA) {
         l.ss = take(L);
         l.st = take(H);
         l.yb = take(H);
     }
     l.total = o;
     return l;
+}
+
+Layout layout_for(const HostPrep &hp) { return layout_for(hp.logl, hp.exp.size()); }
+
+// Slot layout of the server: the exponent region sized for the longest
+// modulus of the length class, so that slots of one class are interchangeable.
+Layout slot_layout(int logl) {
+    const size_t H = (size_t)1 << (logl - 1);
+    return layout_for(logl, (LIMB_BITS * H + 31) / 32 + 1);
 }
 
 void prep_all(const pfb_mr_number_t *nums, int n, uint32_t base, int mode, const pfb_mr_number_t *exps,
@@ -492,6 +550,8 @@ struct pfb_mr_batch {
     long long max_steps = 0, steps_done = 0;
     uint8_t *d_arena = nullptr;
     JobDev *d_jobs = nullptr;
+    int *d_locks = nullptr;           // [n] per-candidate locks of the persistent kernel
+    unsigned int *d_counter = nullptr;  // quanta handed out in the current launch
     std::vector<HostPrep> hp;
     std::vector<JobDev> jobs;
 };
@@ -522,7 +582,8 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
         b->n_ok++;
     }
     const size_t job_bytes = ((size_t)n * sizeof(JobDev) + 255) & ~(size_t)255;
-    const size_t need = job_bytes + total * sizeof(uint32_t);
+    const size_t lock_bytes = ((size_t)n * sizeof(int) + 256 + 255) & ~(size_t)255;
+    const size_t need = job_bytes + lock_bytes + total * sizeof(uint32_t);
     if (cudaMalloc(&b->d_arena, need) != cudaSuccess) {
         cudaGetLastError();
         pfb::set_error("pfb_mr: cannot allocate %zu bytes of device memory", need);
@@ -530,7 +591,14 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
         return PFB_E_NOMEM;
     }
     b->d_jobs = (JobDev *)b->d_arena;
-    uint32_t *d_words = (uint32_t *)(b->d_arena + job_bytes);
+    b->d_locks = (int *)(b->d_arena + job_bytes);
+    b->d_counter = (unsigned int *)(b->d_arena + job_bytes + lock_bytes - 256);
+    uint32_t *d_words = (uint32_t *)(b->d_arena + job_bytes + lock_bytes);
+    if (cudaMemsetAsync(b->d_locks, 0, lock_bytes, e->stream) != cudaSuccess) {
+        cudaFree(b->d_arena);
+        delete b;
+        return pfb::cuda_fail(cudaGetLastError(), "lock reset", __FILE__, __LINE__);
+    }
     b->jobs.assign(n, JobDev{});
     size_t off = 0;
     int rc = PFB_OK;
@@ -576,7 +644,7 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     if (!rc) ce = cudaMemcpyAsync(b->d_jobs, b->jobs.data(), n * sizeof(JobDev), cudaMemcpyHostToDevice, e->stream);
     if (!rc && ce != cudaSuccess) rc = pfb::cuda_fail(ce, "job upload", __FILE__, __LINE__);
     if (!rc && b->n_ok) {
-        prep_kernel<<<n, THREADS, smem_bytes(b->maxlog), e->stream>>>(b->d_jobs, e->tw);
+        prep_kernel<<<n, THREADS, smem_bytes(b->maxlog), e->stream>>>(b->d_jobs, nullptr, e->tw);
         ce = cudaGetLastError();
         if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "prep_kernel", __FILE__, __LINE__);
     }
@@ -594,17 +662,39 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     return PFB_OK;
 }
 
+// Enqueues about `steps` steps of every unfinished candidate: launches of the
+// persistent kernel, each handing out n * ceil(chunk / quantum) quanta.
 int batch_advance(pfb_mr_batch *b, long long steps, cudaStream_t st) {
-    if (!b->n_ok) return PFB_OK;
+    if (!b->n_ok || steps <= 0) return PFB_OK;
     const size_t sm = smem_bytes(b->maxlog);
-    const int chunk = 2048;
+    const int grid = std::min(b->n, std::max(1, b->e->num_sms));
     while (steps > 0) {
-        const int k = (int)std::min<long long>(steps, chunk);
-        step_kernel<<<b->n, THREADS, sm, st>>>(b->d_jobs, k, b->e->tw);
+        const long long chunk = std::min<long long>(steps, 2048);
+        const int quantum = (int)std::min<long long>(chunk, 64);
+        const long long qpj = (chunk + quantum - 1) / quantum;
+        const unsigned int total = (unsigned int)std::min<long long>((long long)b->n * qpj, 0x7fffffffll);
+        PFB_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned int), st));
+        persist_kernel<<<grid, THREADS, sm, st>>>(b->d_jobs, b->n, b->d_locks, b->d_counter, total, quantum,
+                                                  b->e->tw);
         PFB_CUDA(cudaGetLastError());
-        steps -= k;
-        b->steps_done += k;
+        steps -= chunk;
+        b->steps_done += chunk;
     }
+    return PFB_OK;
+}
+
+int batch_pending(pfb_mr_batch *b, int *pending, long long *steps_total) {
+    PFB_CUDA(cudaStreamSynchronize(b->e->stream));
+    PFB_CUDA(cudaDeviceSynchronize());
+    PFB_CUDA(cudaMemcpy(b->jobs.data(), b->d_jobs, b->n * sizeof(JobDev), cudaMemcpyDeviceToHost));
+    int c = 0;
+    long long st = 0;
+    for (int i = 0; i < b->n; i++) {
+        c += b->jobs[i].phase != 3;
+        st += b->jobs[i].steps;
+    }
+    if (pending) *pending = c;
+    if (steps_total) *steps_total = st;
     return PFB_OK;
 }
 
@@ -649,6 +739,13 @@ int run_jobs(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int m
     int rc = batch_build(e, nums, n, base, mode, exps, &b);
     if (rc) return rc;
     rc = batch_advance(b, b->max_steps, e->stream);
+    // The round-robin hands a locked candidate's quantum to another one, so a
+    // few candidates may still need steps: continue until none is pending.
+    for (int pending = 1; !rc;) {
+        rc = batch_pending(b, &pending, nullptr);
+        if (rc || pending == 0) break;
+        rc = batch_advance(b, 4096, e->stream);
+    }
     if (!rc) rc = batch_results(b, verdict, residue, residue_stride);
     cudaStreamSynchronize(e->stream);
     cudaFree(b->d_arena);
@@ -696,12 +793,15 @@ extern "C" int pfb_mr_batch_pending(pfb_mr_batch_t *b, int *pending) {
         return PFB_E_ARG;
     }
     PFB_CUDA(cudaSetDevice(b->e->device));
-    PFB_CUDA(cudaDeviceSynchronize());
-    PFB_CUDA(cudaMemcpy(b->jobs.data(), b->d_jobs, b->n * sizeof(JobDev), cudaMemcpyDeviceToHost));
-    int c = 0;
-    for (int i = 0; i < b->n; i++) c += b->jobs[i].phase != 3;
-    *pending = c;
-    return PFB_OK;
+    return batch_pending(b, pending, nullptr);
+}
+
+extern "C" long long pfb_mr_batch_steps_done(pfb_mr_batch_t *b) {
+    if (!b) return -1;
+    if (cudaSetDevice(b->e->device) != cudaSuccess) return -1;
+    long long st = 0;
+    if (batch_pending(b, nullptr, &st)) return -1;
+    return st;
 }
 
 extern "C" long long pfb_mr_batch_steps_left(pfb_mr_batch_t *b) {
@@ -733,4 +833,459 @@ extern "C" long long pfb_mr_test_cost(const uint16_t *limbs, int n_limbs) {
     const size_t nb = pfb::big::bit_length(N);
     if (nb < 2) return -1;
     return (long long)nb;  // ~ bits(d) squarings + one conversion
+}
+
+// ===========================================================================
+// Serving: continuous batching on one GPU.
+//
+// Requests (candidates of any length) are prepared on host worker threads
+// (N', R mod N, exponent) and admitted into free slots of a device-resident
+// job table between launches of the persistent kernel, as slots and the HBM
+// budget allow; every launch advances all resident candidates, whatever
+// their lengths, round-robin by quanta; finished candidates are retired with
+// their timestamps and their slot memory returns to a size-class pool.  All
+// host waits are bounded (condition variables with timeouts); nothing on the
+// device waits.
+
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct SrvRequest {
+    uint64_t tag = 0;
+    std::vector<uint16_t> limbs;
+    uint16_t *residue_out = nullptr;
+    int residue_cap = 0;
+    double t_submit = 0.0, t_admit = 0.0;
+    HostPrep hp;
+};
+
+struct SrvSlot {
+    bool busy = false;
+    int logl = 0;
+    uint8_t *mem = nullptr;
+    SrvRequest req;
+};
+
+}  // namespace
+
+struct pfb_mr_server {
+    pfb_mr *e = nullptr;
+    pfb_mr_server_config_t cfg{};
+    Clock::time_point t0;
+    // device job table
+    JobDev *d_jobs = nullptr;
+    int *d_locks = nullptr;
+    unsigned int *d_counter = nullptr;
+    int *d_list = nullptr;
+    uint8_t *d_table_mem = nullptr;
+    std::vector<JobDev> jobs;
+    std::vector<SrvSlot> slots;
+    std::map<int, std::vector<uint8_t *>> pool;  // free slot memory by transform length
+    size_t bytes_in_use = 0, bytes_owned = 0;
+    cudaStream_t stream = nullptr;
+    // queues
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<SrvRequest> submitted, prepared;
+    std::deque<pfb_mr_result_t> done;
+    bool stop = false;
+    int preparing = 0;
+    // statistics
+    long long n_submitted = 0, n_admitted = 0, n_completed = 0, launches = 0;
+    long long steps_total = 0;
+    int resident = 0;
+    std::vector<std::thread> workers;
+    std::thread driver;
+    int error = PFB_OK;
+};
+
+namespace {
+
+double now_s(const pfb_mr_server *s) {
+    return std::chrono::duration<double>(Clock::now() - s->t0).count();
+}
+
+size_t slot_bytes(int logl) { return slot_layout(logl).total * sizeof(uint32_t); }
+
+void srv_prep_worker(pfb_mr_server *s) {
+    for (;;) {
+        SrvRequest r;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            while (!s->stop && s->submitted.empty()) s->cv_work.wait_for(lk, std::chrono::milliseconds(100));
+            if (s->stop) return;
+            r = std::move(s->submitted.front());
+            s->submitted.pop_front();
+            s->preparing++;
+        }
+        pfb_mr_number_t num{r.limbs.data(), (int)r.limbs.size()};
+        host_prep(num, s->cfg.base, 1, nullptr, r.hp);
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->preparing--;
+            if (!r.hp.ok) {
+                pfb_mr_result_t res{};
+                res.tag = r.tag;
+                res.verdict = -1;
+                res.submit_s = r.t_submit;
+                res.admit_s = res.done_s = now_s(s);
+                s->done.push_back(res);
+                s->n_completed++;
+                s->cv_done.notify_all();
+            } else {
+                s->prepared.push_back(std::move(r));
+            }
+        }
+        s->cv_work.notify_all();
+    }
+}
+
+// Admits prepared requests into free slots; returns the slots admitted.
+int srv_admit(pfb_mr_server *s, std::vector<int> &admitted) {
+    admitted.clear();
+    for (;;) {
+        SrvRequest r;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            if (s->prepared.empty()) break;
+            int free_slot = -1;
+            for (int i = 0; i < (int)s->slots.size(); i++)
+                if (!s->slots[i].busy) {
+                    free_slot = i;
+                    break;
+                }
+            if (free_slot < 0) break;
+            const int lg = s->prepared.front().hp.logl;
+            const size_t need = slot_bytes(lg);
+            const bool pooled = !s->pool[lg].empty();
+            if (s->cfg.hbm_budget_bytes && !pooled && s->bytes_owned + need > s->cfg.hbm_budget_bytes) {
+                // give back pooled blocks of other lengths first
+                for (auto &kv : s->pool) {
+                    while (!kv.second.empty() && s->bytes_owned + need > s->cfg.hbm_budget_bytes) {
+                        const size_t blk = slot_bytes(kv.first);
+                        cudaFree(kv.second.back());
+                        kv.second.pop_back();
+                        s->bytes_owned -= std::min(s->bytes_owned, blk);
+                    }
+                }
+            }
+            if (s->cfg.hbm_budget_bytes && !pooled && s->bytes_owned + need > s->cfg.hbm_budget_bytes) {
+                if (s->resident == 0 && admitted.empty()) {
+                    // a single request above the whole budget can never run
+                    SrvRequest bad = std::move(s->prepared.front());
+                    s->prepared.pop_front();
+                    pfb_mr_result_t res{};
+                    res.tag = bad.tag;
+                    res.verdict = -1;
+                    res.submit_s = bad.t_submit;
+                    res.admit_s = res.done_s = now_s(s);
+                    s->done.push_back(res);
+                    s->n_completed++;
+                    s->cv_done.notify_all();
+                    continue;
+                }
+                break;  // wait for memory to come back
+            }
+            r = std::move(s->prepared.front());
+            s->prepared.pop_front();
+            SrvSlot &sl = s->slots[free_slot];
+            sl.busy = true;
+            sl.logl = lg;
+            if (pooled) {
+                sl.mem = s->pool[lg].back();
+                s->pool[lg].pop_back();
+            } else {
+                sl.mem = nullptr;
+            }
+            s->bytes_in_use += need;
+            admitted.push_back(free_slot);
+            r.t_admit = now_s(s);
+            sl.req = std::move(r);
+        }
+        SrvSlot &sl = s->slots[admitted.back()];
+        if (!sl.mem) {
+            const size_t need = slot_bytes(sl.logl);
+            if (cudaMalloc(&sl.mem, need) != cudaSuccess) {
+                cudaGetLastError();
+                return PFB_E_NOMEM;
+            }
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->bytes_owned += need;
+        }
+        // fill the job and upload its inputs
+        const HostPrep &h = sl.req.hp;
+        const Layout l = slot_layout(h.logl);
+        uint32_t *w = (uint32_t *)sl.mem;
+        JobDev &j = s->jobs[admitted.back()];
+        memset(&j, 0, sizeof(j));
+        j.x = w + l.x;
+        j.res = w + l.res;
+        j.nph = w + l.nph;
+        j.nh = w + l.nh;
+        j.npl = w + l.npl;
+        j.nl = w + l.nl;
+        j.exp = w + l.exp;
+        if (h.logl > LOG_LCTA) {
+            j.spill_s = w + l.ss;
+            j.spill_t = w + l.st;
+            j.ybuf = w + l.yb;
+        }
+        j.logl = h.logl;
+        j.cursor = h.cursor;
+        j.extra = h.s - 1;
+        j.phase = 0;
+        j.base = s->cfg.base;
+        j.mode = 1;
+        const size_t H = h.x0.size();
+        PFB_CUDA(cudaMemcpyAsync(j.x, h.x0.data(), H * 4, cudaMemcpyHostToDevice, s->stream));
+        PFB_CUDA(cudaMemcpyAsync((void *)j.npl, h.npl.data(), H * 4, cudaMemcpyHostToDevice, s->stream));
+        PFB_CUDA(cudaMemcpyAsync((void *)j.nl, h.nl.data(), H * 4, cudaMemcpyHostToDevice, s->stream));
+        PFB_CUDA(cudaMemcpyAsync((void *)j.exp, h.exp.data(), h.exp.size() * 4, cudaMemcpyHostToDevice, s->stream));
+        PFB_CUDA(cudaMemcpyAsync(s->d_jobs + admitted.back(), &j, sizeof(JobDev), cudaMemcpyHostToDevice, s->stream));
+        PFB_CUDA(cudaStreamSynchronize(s->stream));  // host staging is freed below / reused
+    }
+    if (!admitted.empty()) {
+        PFB_CUDA(cudaMemcpyAsync(s->d_list, admitted.data(), admitted.size() * sizeof(int), cudaMemcpyHostToDevice,
+                                 s->stream));
+        int maxlog = LOG_LMIN;
+        for (int i : admitted) maxlog = std::max(maxlog, s->slots[i].logl);
+        prep_kernel<<<(int)admitted.size(), THREADS, smem_bytes(maxlog), s->stream>>>(s->d_jobs, s->d_list, s->e->tw);
+        PFB_CUDA(cudaGetLastError());
+        PFB_CUDA(cudaStreamSynchronize(s->stream));
+        for (int i : admitted) {  // the set-up inputs are on the device now
+            HostPrep &h = s->slots[i].req.hp;
+            std::vector<uint32_t>().swap(h.npl);
+            std::vector<uint32_t>().swap(h.exp);
+        }
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->resident += (int)admitted.size();
+        s->n_admitted += (long long)admitted.size();
+    }
+    return PFB_OK;
+}
+
+// Retires finished candidates (host mirror of the job table already read).
+void srv_retire(pfb_mr_server *s) {
+    std::vector<uint32_t> r22;
+    for (int i = 0; i < (int)s->slots.size(); i++) {
+        SrvSlot &sl = s->slots[i];
+        if (!sl.busy || s->jobs[i].phase != 3) continue;
+        pfb_mr_result_t res{};
+        res.tag = sl.req.tag;
+        res.verdict = (int8_t)s->jobs[i].verdict;
+        res.submit_s = sl.req.t_submit;
+        res.admit_s = sl.req.t_admit;
+        if (sl.req.residue_out && sl.req.residue_cap > 0) {
+            const size_t H = sl.req.hp.x0.size();
+            r22.resize(H);
+            if (cudaMemcpy(r22.data(), s->jobs[i].res, H * 4, cudaMemcpyDeviceToHost) == cudaSuccess) {
+                pfb::big::Words r = pfb::big::from_limbs(r22.data(), LIMB_BITS, H);
+                pfb::big::to_u16(r, sl.req.residue_out, (size_t)sl.req.residue_cap);
+            }
+        }
+        res.done_s = now_s(s);
+        const size_t bytes = slot_bytes(sl.logl);
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->pool[sl.logl].push_back(sl.mem);
+        sl.mem = nullptr;
+        sl.busy = false;
+        s->bytes_in_use -= bytes;
+        s->resident--;
+        s->n_completed++;
+        s->steps_total += s->jobs[i].steps;
+        s->done.push_back(res);
+        s->cv_done.notify_all();
+    }
+}
+
+void srv_driver(pfb_mr_server *s) {
+    if (cudaSetDevice(s->e->device) != cudaSuccess) {
+        s->error = PFB_E_CUDA;
+        return;
+    }
+    std::vector<int> admitted;
+    const int cap = (int)s->slots.size();
+    const int grid_max = std::max(1, s->e->num_sms);
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            while (!s->stop && s->resident == 0 && s->prepared.empty())
+                s->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+            if (s->stop) break;
+        }
+        int rc = srv_admit(s, admitted);
+        if (rc) {
+            s->error = rc;
+            break;
+        }
+        int res_now;
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            res_now = s->resident;
+        }
+        if (res_now == 0) continue;
+        // one launch: every resident candidate advances about chunk_steps steps
+        const int quantum = std::min(64, s->cfg.chunk_steps);
+        const long long qpj = (s->cfg.chunk_steps + quantum - 1) / quantum;
+        int maxlog = LOG_LMIN;
+        for (auto &sl : s->slots)
+            if (sl.busy) maxlog = std::max(maxlog, sl.logl);
+        cudaMemsetAsync(s->d_counter, 0, sizeof(unsigned int), s->stream);
+        persist_kernel<<<std::min(res_now, grid_max), THREADS, smem_bytes(maxlog), s->stream>>>(
+            s->d_jobs, cap, s->d_locks, s->d_counter, (unsigned int)(res_now * qpj), quantum, s->e->tw);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(s->jobs.data(), s->d_jobs, cap * sizeof(JobDev), cudaMemcpyDeviceToHost, s->stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(s->stream) != cudaSuccess) {
+            pfb::set_error("pfb_mr_server: CUDA failure in the step loop");
+            s->error = PFB_E_CUDA;
+            break;
+        }
+        s->launches++;
+        srv_retire(s);
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stop = true;
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+}
+
+}  // namespace
+
+extern "C" int pfb_mr_server_create(pfb_mr_t *e, const pfb_mr_server_config_t *cfg, pfb_mr_server_t **out) {
+    if (!e || !out) {
+        pfb::set_error("pfb_mr_server_create: null argument");
+        return PFB_E_ARG;
+    }
+    *out = nullptr;
+    pfb_mr_server *s = new pfb_mr_server();
+    s->e = e;
+    if (cfg) s->cfg = *cfg;
+    if (s->cfg.max_resident <= 0) s->cfg.max_resident = 2 * std::max(1, e->num_sms);
+    if (s->cfg.chunk_steps <= 0) s->cfg.chunk_steps = 512;
+    if (s->cfg.base < 2 || s->cfg.base > 0xFFFFu) s->cfg.base = 2;
+    if (s->cfg.prep_threads <= 0) s->cfg.prep_threads = 4;
+    s->t0 = Clock::now();
+    const int cap = s->cfg.max_resident;
+    PFB_CUDA(cudaSetDevice(e->device));
+    const size_t job_bytes = ((size_t)cap * sizeof(JobDev) + 255) & ~(size_t)255;
+    const size_t int_bytes = ((size_t)cap * sizeof(int) + 255) & ~(size_t)255;
+    if (cudaMalloc(&s->d_table_mem, job_bytes + 2 * int_bytes + 256) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        pfb::set_error("pfb_mr_server_create: cannot allocate the job table");
+        return PFB_E_NOMEM;
+    }
+    s->d_jobs = (JobDev *)s->d_table_mem;
+    s->d_locks = (int *)(s->d_table_mem + job_bytes);
+    s->d_list = (int *)(s->d_table_mem + job_bytes + int_bytes);
+    s->d_counter = (unsigned int *)(s->d_table_mem + job_bytes + 2 * int_bytes);
+    s->jobs.assign(cap, JobDev{});
+    for (auto &j : s->jobs) j.phase = 3;
+    s->slots.resize(cap);
+    int rc = PFB_OK;
+    cudaError_t ce = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaMemcpy(s->d_jobs, s->jobs.data(), cap * sizeof(JobDev), cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess) ce = cudaMemset(s->d_locks, 0, int_bytes);
+    if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "server set-up", __FILE__, __LINE__);
+    if (rc) {
+        cudaFree(s->d_table_mem);
+        if (s->stream) cudaStreamDestroy(s->stream);
+        delete s;
+        return rc;
+    }
+    for (int t = 0; t < s->cfg.prep_threads; t++) s->workers.emplace_back(srv_prep_worker, s);
+    s->driver = std::thread(srv_driver, s);
+    *out = s;
+    return PFB_OK;
+}
+
+extern "C" int pfb_mr_server_submit(pfb_mr_server_t *s, const uint16_t *limbs, int n_limbs, uint64_t tag,
+                                    uint16_t *residue_out, int residue_cap) {
+    if (!s || !limbs || n_limbs <= 0 || (residue_out && residue_cap <= 0)) {
+        pfb::set_error("pfb_mr_server_submit: bad argument");
+        return PFB_E_ARG;
+    }
+    SrvRequest r;
+    r.tag = tag;
+    r.limbs.assign(limbs, limbs + n_limbs);
+    r.residue_out = residue_out;
+    r.residue_cap = residue_cap;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            pfb::set_error("pfb_mr_server_submit: server stopped (%d)", s->error);
+            return PFB_E_STATE;
+        }
+        r.t_submit = now_s(s);
+        s->submitted.push_back(std::move(r));
+        s->n_submitted++;
+    }
+    s->cv_work.notify_all();
+    return PFB_OK;
+}
+
+extern "C" int pfb_mr_server_poll(pfb_mr_server_t *s, pfb_mr_result_t *out, int cap, int timeout_ms) {
+    if (!s || !out || cap <= 0) {
+        pfb::set_error("pfb_mr_server_poll: bad argument");
+        return PFB_E_ARG;
+    }
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->done.empty() && timeout_ms > 0 && !s->stop)
+        s->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return !s->done.empty() || s->stop; });
+    int n = 0;
+    while (n < cap && !s->done.empty()) {
+        out[n++] = s->done.front();
+        s->done.pop_front();
+    }
+    if (n == 0 && s->stop && s->error) return s->error;
+    return n;
+}
+
+extern "C" int pfb_mr_server_stats(pfb_mr_server_t *s, pfb_mr_server_stats_t *st) {
+    if (!s || !st) {
+        pfb::set_error("pfb_mr_server_stats: bad argument");
+        return PFB_E_ARG;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    st->submitted = s->n_submitted;
+    st->admitted = s->n_admitted;
+    st->completed = s->n_completed;
+    st->resident = s->resident;
+    st->queued = (int)(s->submitted.size() + s->prepared.size()) + s->preparing;
+    st->launches = s->launches;
+    st->steps_retired = s->steps_total;
+    st->bytes_in_use = s->bytes_in_use;
+    st->bytes_owned = s->bytes_owned;
+    st->error = s->error;
+    return PFB_OK;
+}
+
+extern "C" void pfb_mr_server_destroy(pfb_mr_server_t *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    s->cv_done.notify_all();
+    if (s->driver.joinable()) s->driver.join();
+    for (auto &t : s->workers)
+        if (t.joinable()) t.join();
+    cudaSetDevice(s->e->device);
+    cudaStreamSynchronize(s->stream);
+    for (auto &sl : s->slots)
+        if (sl.mem) cudaFree(sl.mem);
+    for (auto &kv : s->pool)
+        for (uint8_t *m : kv.second) cudaFree(m);
+    cudaFree(s->d_table_mem);
+    cudaStreamDestroy(s->stream);
+    delete s;
 }

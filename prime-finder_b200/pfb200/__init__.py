@@ -399,3 +399,106 @@ def build_candidate(a: int, b: int, c: int, k: int, j: int, rev: bool = False) -
         lk, lj = ndigits(k), ndigits(j)
         return 10 ** a - rev_digits(k, lk) * 10 ** (a - b - lk) - rev_digits(j, lj) * 10 ** (a - c - lj) - 1
     return 10 ** a - k * 10 ** b - j * 10 ** c - 1
+
+
+# ----------------------------------------------------------------- serving ---
+
+class ServerConfig(C.Structure):
+    """pfb_mr_server_config_t"""
+    _fields_ = [("max_resident", C.c_int), ("hbm_budget_bytes", C.c_size_t), ("chunk_steps", C.c_int),
+                ("base", C.c_uint32), ("prep_threads", C.c_int)]
+
+
+class ServerResult(C.Structure):
+    """pfb_mr_result_t"""
+    _fields_ = [("tag", C.c_uint64), ("verdict", C.c_int8), ("submit_s", C.c_double),
+                ("admit_s", C.c_double), ("done_s", C.c_double)]
+
+
+class ServerStats(C.Structure):
+    """pfb_mr_server_stats_t"""
+    _fields_ = [("submitted", C.c_longlong), ("admitted", C.c_longlong), ("completed", C.c_longlong),
+                ("launches", C.c_longlong), ("steps_retired", C.c_longlong), ("resident", C.c_int),
+                ("queued", C.c_int), ("error", C.c_int), ("bytes_in_use", C.c_size_t),
+                ("bytes_owned", C.c_size_t)]
+
+
+def _server_lib():
+    L = _batch_lib()
+    if not hasattr(L, "_server_ready"):
+        vp = C.c_void_p
+        L.pfb_mr_server_create.argtypes = [vp, C.POINTER(ServerConfig), C.POINTER(vp)]
+        L.pfb_mr_server_create.restype = C.c_int
+        L.pfb_mr_server_submit.argtypes = [vp, C.POINTER(C.c_uint16), C.c_int, C.c_uint64,
+                                           C.POINTER(C.c_uint16), C.c_int]
+        L.pfb_mr_server_submit.restype = C.c_int
+        L.pfb_mr_server_poll.argtypes = [vp, C.POINTER(ServerResult), C.c_int, C.c_int]
+        L.pfb_mr_server_poll.restype = C.c_int
+        L.pfb_mr_server_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        L.pfb_mr_server_stats.restype = C.c_int
+        L.pfb_mr_server_destroy.argtypes = [vp]
+        L.pfb_mr_server_destroy.restype = None
+        L.pfb_mr_batch_steps_done.argtypes = [vp]
+        L.pfb_mr_batch_steps_done.restype = C.c_longlong
+        L._server_ready = True
+    return L
+
+
+class MRServer:
+    """Continuous-batching strong-test server (pfb_mr_server_* C ABI)."""
+
+    def __init__(self, engine: "MillerRabin", max_resident: int = 0, hbm_budget_bytes: int = 0,
+                 chunk_steps: int = 0, base: int = 2, prep_threads: int = 0):
+        L = _server_lib()
+        self._cfg = ServerConfig(max_resident, hbm_budget_bytes, chunk_steps, base, prep_threads)
+        h = C.c_void_p()
+        _check(L.pfb_mr_server_create(engine._h, C.byref(self._cfg), C.byref(h)), "pfb_mr_server_create")
+        self._h = h
+        self._bufs = {}   # tag -> (limbs, residue buffer) kept alive until the result is read
+
+    def submit(self, number, tag: int, residue: bool = False) -> None:
+        limbs = number if isinstance(number, np.ndarray) else int_to_limbs16(int(number))
+        limbs = np.ascontiguousarray(limbs, dtype=np.uint16)
+        res = np.zeros(len(limbs), dtype=np.uint16) if residue else None
+        self._bufs[tag] = (limbs, res)
+        rc = _server_lib().pfb_mr_server_submit(
+            self._h, limbs.ctypes.data_as(C.POINTER(C.c_uint16)), len(limbs), tag,
+            res.ctypes.data_as(C.POINTER(C.c_uint16)) if residue else None, len(limbs) if residue else 0)
+        _check(rc, "pfb_mr_server_submit")
+
+    def poll(self, cap: int = 64, timeout_ms: int = 100):
+        """List of dicts {tag, verdict, submit_s, admit_s, done_s[, residue]}."""
+        out = (ServerResult * cap)()
+        n = _server_lib().pfb_mr_server_poll(self._h, out, cap, timeout_ms)
+        if n < 0:
+            raise PfbError(n, "pfb_mr_server_poll")
+        res = []
+        for i in range(n):
+            r = out[i]
+            d = {"tag": int(r.tag), "verdict": int(r.verdict), "submit_s": r.submit_s,
+                 "admit_s": r.admit_s, "done_s": r.done_s}
+            limbs, rb = self._bufs.pop(int(r.tag), (None, None))
+            if rb is not None:
+                d["residue"] = limbs16_to_int(rb)
+            res.append(d)
+        return res
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(_server_lib().pfb_mr_server_stats(self._h, C.byref(st)), "pfb_mr_server_stats")
+        return {f: getattr(st, f) for f, _ in ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _server_lib().pfb_mr_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def batch_steps_done(batch: "MRBatch") -> int:
+    return int(_server_lib().pfb_mr_batch_steps_done(batch._h))

@@ -1,0 +1,91 @@
+"""Continuous batching: results are the same alone and in the mix.
+
+Candidates of different lengths are streamed into the server while others
+are resident (staggered submission), and each verdict and residue must equal
+the one-candidate-per-call result and GMP's (oracle), word for word.
+"""
+import random
+import time
+
+import pytest
+
+import oracle
+import pfb200
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def engine():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    e = pfb200.MillerRabin(0)
+    yield e
+    e.close()
+
+
+def _numbers(seed, n):
+    rng = random.Random(seed)
+    out = []
+    for i in range(n):
+        bits = rng.choice([700, 1500, 3000, 2790, 6000, 9000, 12000])
+        out.append(rng.getrandbits(bits) | (1 << (bits - 1)) | 1)
+    out[3] = (1 << 1279) - 1          # a prime (passes)
+    out[5] = oracle.nextprime(1 << 700)
+    return out
+
+
+def _drain(srv, want, timeout_s=120):
+    got = {}
+    t0 = time.time()
+    while len(got) < want and time.time() - t0 < timeout_s:
+        for r in srv.poll(64, 200):
+            got[r["tag"]] = r
+    return got
+
+
+def test_alone_equals_in_the_mix(engine):
+    Ns = _numbers(1, 24)
+    alone = [engine.test([N], 2) for N in Ns]          # one candidate per call
+    srv = pfb200.MRServer(engine, max_resident=6, chunk_steps=256)
+    got = {}
+    for i, N in enumerate(Ns):                       # arrivals while others run
+        srv.submit(N, tag=i, residue=True)
+        if i % 5 == 4:
+            time.sleep(0.05)
+            for r in srv.poll(64, 10):
+                got[r["tag"]] = r
+    got.update(_drain(srv, len(Ns) - len(got)))
+    st = srv.stats()
+    srv.close()
+    assert len(got) == len(Ns), st
+    for i, N in enumerate(Ns):
+        v_alone, r_alone = alone[i][0][0], alone[i][1][0]
+        assert got[i]["verdict"] == v_alone == oracle.strong_test(N, 2)
+        assert got[i]["residue"] == r_alone == oracle.strong_residue(N, 2)[1]
+        assert got[i]["submit_s"] <= got[i]["admit_s"] <= got[i]["done_s"]
+    assert st["launches"] > 1 and st["completed"] == len(Ns)
+
+
+def test_budget_limits_admission(engine):
+    Ns = _numbers(2, 8)
+    srv = pfb200.MRServer(engine, max_resident=8, hbm_budget_bytes=150_000, chunk_steps=128)
+    for i, N in enumerate(Ns):
+        srv.submit(N, tag=i, residue=True)
+    got = _drain(srv, len(Ns))
+    st = srv.stats()
+    srv.close()
+    assert st["bytes_owned"] <= 150_000 and st["completed"] == len(Ns)
+    for i, N in enumerate(Ns):
+        assert got[i]["residue"] == oracle.strong_residue(N, 2)[1]
+
+
+def test_invalid_requests_reported(engine):
+    srv = pfb200.MRServer(engine, max_resident=2)
+    srv.submit(10, tag=1)
+    srv.submit(1 << 400, tag=2)
+    srv.submit(2047, tag=3)   # base-2 strong pseudoprime
+    got = _drain(srv, 3, 60)
+    srv.close()
+    assert got[1]["verdict"] == -1 and got[2]["verdict"] == -1 and got[3]["verdict"] == 1
