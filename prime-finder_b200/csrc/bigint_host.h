@@ -229,5 +229,72 @@ inline Words pow2_mod(size_t e, const Words &N) {
     return out;
 }
 
+// a * b, schoolbook.
+inline Words mul(const Words &a, const Words &b) {
+    if (a.empty() || b.empty()) return Words();
+    Words r(a.size() + b.size(), 0);
+    for (size_t i = 0; i < a.size(); i++) {
+        unsigned __int128 carry = 0;
+        const uint64_t ai = a[i];
+        for (size_t j = 0; j < b.size(); j++) {
+            unsigned __int128 t = (unsigned __int128)ai * b[j] + r[i + j] + carry;
+            r[i + j] = (uint64_t)t;
+            carry = t >> 64;
+        }
+        r[i + b.size()] = (uint64_t)carry;
+    }
+    trim(r);
+    return r;
+}
+
+inline Words mul_small(const Words &a, uint64_t m) {
+    Words r(a.size() + 1, 0);
+    unsigned __int128 carry = 0;
+    for (size_t i = 0; i < a.size(); i++) {
+        unsigned __int128 t = (unsigned __int128)a[i] * m + carry;
+        r[i] = (uint64_t)t;
+        carry = t >> 64;
+    }
+    r[a.size()] = (uint64_t)carry;
+    trim(r);
+    return r;
+}
+
+inline Words shl(const Words &a, size_t s) {
+    if (a.empty()) return a;
+    const size_t ws = s / 64, bs = s % 64;
+    Words r(a.size() + ws + 1, 0);
+    for (size_t i = 0; i < a.size(); i++) {
+        r[i + ws] |= a[i] << bs;
+        if (bs) r[i + ws + 1] |= a[i] >> (64 - bs);
+    }
+    trim(r);
+    return r;
+}
+
+// a - b for a >= b.
+inline Words sub(const Words &a, const Words &b) {
+    Words r = a;
+    uint64_t borrow = 0;
+    for (size_t i = 0; i < r.size(); i++) {
+        const uint64_t bi = i < b.size() ? b[i] : 0;
+        const unsigned __int128 d = (unsigned __int128)r[i] - bi - borrow;
+        r[i] = (uint64_t)d;
+        borrow = (uint64_t)(d >> 127);  // 1 when the subtraction wrapped
+    }
+    trim(r);
+    return r;
+}
+
+// 10^e = 5^e * 2^e (square-and-multiply on 5^e).
+inline Words pow10(uint64_t e) {
+    Words r(1, 1), x(1, 5);
+    for (uint64_t k = e; k; k >>= 1) {
+        if (k & 1) r = mul(r, x);
+        if (k > 1) x = mul(x, x);
+    }
+    return shl(r, e);
+}
+
 }  // namespace big
 }  // namespace pfb
