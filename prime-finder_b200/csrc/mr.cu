@@ -48,7 +48,7 @@ struct JobDev {
 // transform + X above (the sequential-prime step keeps Y in global memory).
 __host__ __device__ inline size_t smem_words(int logl) {
     const size_t L = (size_t)1 << logl, H = L / 2;
-    return logl <= LOG_LCTA ? 2 * (L + L / 32) + 2 * H : (L + L / 32) + H;
+    return logl <= LOG_LCTA ? 2 * (L + L / 32) + 2 * (H + H / 32) : (L + L / 32) + (H + H / 32);
 }
 inline size_t smem_bytes(int logl) {
     return smem_words(logl) * sizeof(uint32_t) + sizeof(CarrySmem) + 16;
@@ -60,7 +60,7 @@ __device__ __forceinline__ void carve(uint32_t *raw, int logl, Smem &sm, uint32_
     if (logl <= LOG_LCTA) {
         sm.A1 = raw + L + L / 32;
         sm.X = sm.A1 + L + L / 32;
-        Y = sm.X + H;
+        Y = sm.X + H + H / 32;
     } else {
         sm.A1 = nullptr;
         sm.X = raw + L + L / 32;
@@ -137,7 +137,7 @@ __device__ __forceinline__ void mstep(const Smem &sm, const Cand &cd, bool squar
 __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uint32_t *nl, const Twiddles &tw,
                           const JobDev &jb) {
     const int H = 1 << (cd.logl - 1);
-    for (int i = threadIdx.x; i < H; i += blockDim.x) Y[i] = sm.X[i];
+    for (int i = threadIdx.x; i < H; i += blockDim.x) Y[pad(i)] = sm.X[pad(i)];
     __syncthreads();
     Smem s2 = sm;
     s2.X = Y;
@@ -145,9 +145,9 @@ __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uin
     // REDC(X) lies in [0, N]; it is N only when X == 0 (mod N), e.g. a base
     // that is a multiple of N.  Map it to 0.
     bool eqn = true;
-    for (int i = threadIdx.x; i < H; i += blockDim.x) eqn = eqn && (Y[i] == nl[i]);
+    for (int i = threadIdx.x; i < H; i += blockDim.x) eqn = eqn && (Y[pad(i)] == nl[i]);
     if (__syncthreads_and(eqn))
-        for (int i = threadIdx.x; i < H; i += blockDim.x) Y[i] = 0u;
+        for (int i = threadIdx.x; i < H; i += blockDim.x) Y[pad(i)] = 0u;
     __syncthreads();
 }
 
@@ -168,7 +168,7 @@ __device__ void run_job(JobDev *jp, int max_steps, const Twiddles &tw, uint32_t 
     carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int H = 1 << (jb.logl - 1);
     const Cand cd{jb.nph, jb.nh, jb.logl};
-    for (int i = threadIdx.x; i < H; i += blockDim.x) sm.X[i] = __ldcg(jb.x + i);
+    for (int i = threadIdx.x; i < H; i += blockDim.x) sm.X[pad(i)] = __ldcg(jb.x + i);
     __syncthreads();
 
     int cursor = jb.cursor, phase = jb.phase, extra = jb.extra, verdict = jb.verdict, steps = 0;
@@ -187,14 +187,14 @@ __device__ void run_job(JobDev *jp, int max_steps, const Twiddles &tw, uint32_t 
             // compare with 1 and N - 1 (N odd: N - 1 differs from N in limb 0 only)
             bool one = true, nm1 = true;
             for (int i = threadIdx.x; i < H; i += blockDim.x) {
-                const uint32_t y = Y[i], nli = jb.nl[i];
+                const uint32_t y = Y[pad(i)], nli = jb.nl[i];
                 one = one && (y == (i == 0 ? 1u : 0u));
                 nm1 = nm1 && (y == (i == 0 ? nli - 1u : nli));
             }
             const int all_one = __syncthreads_and(one);
             const int all_nm1 = __syncthreads_and(nm1);
             if (phase == 1)
-                for (int i = threadIdx.x; i < H; i += blockDim.x) jb.res[i] = Y[i];
+                for (int i = threadIdx.x; i < H; i += blockDim.x) jb.res[i] = Y[pad(i)];
             if (jb.mode == 0) {
                 phase = 3;
             } else if (all_nm1 || (phase == 1 && all_one)) {
@@ -209,7 +209,7 @@ __device__ void run_job(JobDev *jp, int max_steps, const Twiddles &tw, uint32_t 
         }
         steps++;
     }
-    for (int i = threadIdx.x; i < H; i += blockDim.x) jb.x[i] = sm.X[i];
+    for (int i = threadIdx.x; i < H; i += blockDim.x) jb.x[i] = sm.X[pad(i)];
     if (threadIdx.x == 0) {
         jp->cursor = cursor;
         jp->phase = phase;
@@ -509,7 +509,7 @@ Layout layout_for(int logl, size_t exp_words) {
     if (logl > LOG_LCTA) {
         l.ss = take(L);
         l.st = take(H);
-        l.yb = take(H);
+        l.yb = take(H + H / 32);  // padded like the shared-memory residue
     }
     l.total = o;
     return l;

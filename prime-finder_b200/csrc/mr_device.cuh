@@ -482,7 +482,7 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
 
     if (square) {
         for (int i = tid; i < L; i += T) {
-            const uint32_t v = i < H ? X[i] : 0u;
+            const uint32_t v = i < H ? X[pad(i)] : 0u;
             A0[pad(i)] = v;
             A1[pad(i)] = v;
         }
@@ -499,7 +499,7 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
         // T = x^2 as L limbs, in place over A0
         carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
         // S1 = T_lo + T_hi  -> X, carry cS
-        cS = carry_pass<false>(H, 0ull,
+        cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A0[pad(i)] + A0[pad(i + H)]; }, X, cs);
         for (int i = tid; i < L; i += T) {
             const int q = pad(i);
@@ -509,7 +509,7 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
         __syncthreads();
     } else {
         for (int i = tid; i < L; i += T) {
-            const uint32_t v = i < H ? X[i] : 0u;
+            const uint32_t v = i < H ? X[pad(i)] : 0u;
             A0[pad(i)] = v;
             A1[pad(i)] = v;
         }
@@ -529,13 +529,13 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
     const unsigned long long cW =
         carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl - 1, cc); }, A0, cs);
     // U = S1 + W (mod R - 1); S1 = X (square = false: S1 = x itself)
-    unsigned long long c = carry_pass<false>(
-        H, cS + cW, [&](int i) { return (unsigned long long)X[i] + A0[pad(i)]; }, X, cs);
+    unsigned long long c = carry_pass<true>(
+        H, cS + cW, [&](int i) { return (unsigned long long)X[pad(i)] + A0[pad(i)]; }, X, cs);
     while (c) {  // end-around carry: B^H == 1 (mod R - 1); at most two rounds
-        c = carry_pass<false>(H, c, [&](int i) { return (unsigned long long)X[i]; }, X, cs);
+        c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
     }
     if (a > 1u) {
-        carry_pass<false>(H, 0ull, [&](int i) { return (unsigned long long)X[i] * a; }, X, cs);
+        carry_pass<true>(H, 0ull, [&](int i) { return (unsigned long long)X[pad(i)] * a; }, X, cs);
     }
 }
 
@@ -558,7 +558,7 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     const int tid = threadIdx.x, T = blockDim.x;
     unsigned long long cS = 0;
     auto load_x = [&](const uint32_t *src, bool from_global) {
-        for (int i = tid; i < L; i += T) A[pad(i)] = i < H ? (from_global ? ldg_spill(src + i) : src[i]) : 0u;
+        for (int i = tid; i < L; i += T) A[pad(i)] = i < H ? (from_global ? ldg_spill(src + i) : src[pad(i)]) : 0u;
         __syncthreads();
     };
     auto spill = [&](int n) {
@@ -584,13 +584,13 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
         __syncthreads();
         dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
         carry_pass<true>(L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
-        cS = carry_pass<false>(H, 0ull,
+        cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
         for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
         for (int i = H + tid; i < L; i += T) A[pad(i)] = 0u;
         __syncthreads();
     } else {
-        for (int i = tid; i < H; i += T) sp.t[i] = X[i];
+        for (int i = tid; i < H; i += T) sp.t[i] = X[pad(i)];
         load_x(X, false);
     }
     // m = T_lo * N' mod R
@@ -617,10 +617,10 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     dit1<1>(A, logl - 1, tw.wi[1], tw.wish[1]);
     const unsigned long long cW = carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl - 1, cc); }, A, cs);
-    unsigned long long c = carry_pass<false>(
-        H, cS + cW, [&](int i) { return (unsigned long long)X[i] + A[pad(i)]; }, X, cs);
-    while (c) c = carry_pass<false>(H, c, [&](int i) { return (unsigned long long)X[i]; }, X, cs);
-    if (a > 1u) carry_pass<false>(H, 0ull, [&](int i) { return (unsigned long long)X[i] * a; }, X, cs);
+    unsigned long long c = carry_pass<true>(
+        H, cS + cW, [&](int i) { return (unsigned long long)X[pad(i)] + A[pad(i)]; }, X, cs);
+    while (c) c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
+    if (a > 1u) carry_pass<true>(H, 0ull, [&](int i) { return (unsigned long long)X[pad(i)] * a; }, X, cs);
 }
 
 }  // namespace mr
