@@ -37,18 +37,9 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "prime-finder_b200"))
 sys.set_int_max_str_digits(0)
+from pfb200.workloads import serving_draw, sieve_triples, uneven_tuples, uniform_batch_pairs  # noqa: E402
 
 SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference count)
-
-
-def splitmix64(seed):
-    x = seed & (2**64 - 1)
-    while True:
-        x = (x + 0x9E3779B97F4A7C15) & (2**64 - 1)
-        z = x
-        z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & (2**64 - 1)
-        z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & (2**64 - 1)
-        yield z ^ (z >> 31)
 
 
 def ref_modmuls_per_squaring(digits: int) -> int:
@@ -190,29 +181,6 @@ def cpu_sieve_baseline(procs=None, frac=0.05):
                       "one process per core, scaled by prime count" % int(frac * 100)}
 
 
-# ------------------------------------------------------------ workloads ----
-
-def config3_pairs(survivors):
-    g = splitmix64(1)
-    return [survivors[next(g) % len(survivors)] for _ in range(128)]
-
-
-def config2_triples(n):
-    """(a,b,c) of the config-2 enumeration: a in [50000, 50063]; per a, c = 100,
-    b = c+1, c+1+997, ...; the first n triples taken a-major over b."""
-    out = []
-    i = 0
-    while len(out) < n:
-        a = 50000 + (i % 64)
-        bi = i // 64
-        c = 100
-        b = c + 1 + 997 * bi
-        if b <= a - 1:
-            out.append((a, b, c))
-        i += 1
-    return out
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -223,6 +191,7 @@ def main():
     ap.add_argument("--e2e-batch", type=int, default=0, help="candidates in the e2e call (0 = one per SM)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true", help="skip the 512-candidate uneven batch")
     ap.add_argument("--sieve-triples", type=int, default=4)
     ap.add_argument("--serve-secs", type=float, default=0.0,
                     help="also run the serving loop (Poisson arrivals, config 5 shapes) this long")
@@ -243,7 +212,7 @@ def main():
         t0 = time.perf_counter()
         steps = []
         for _ in range(args.warmup + args.steps):
-            steps.append(cpu_mr_baseline(config3_pairs(pairs), abc1, sample_bits=1024))
+            steps.append(cpu_mr_baseline(uniform_batch_pairs(pairs), abc1, sample_bits=1024))
         vals = [s["value"] for s in steps[args.warmup:]]
         v = statistics.mean(vals)
         last = steps[-1]
@@ -265,7 +234,7 @@ def main():
         import json as _j
         g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_config1.json")))
         pairs = [tuple(x) for x in g["survivors_99"]]
-        cpu = cpu_mr_baseline(config3_pairs(pairs), abc1, sample_bits=4096)
+        cpu = cpu_mr_baseline(uniform_batch_pairs(pairs), abc1, sample_bits=4096)
         cpu_sieve = cpu_sieve_baseline()
 
     import numpy as np
@@ -315,7 +284,7 @@ def main():
     dmask = torch.zeros(blk * ntr, dtype=torch.uint8, device="cuda")
     sieve_launches = 0
     with torch.cuda.stream(stream):
-        triples = config2_triples(ntr * (args.steps + args.warmup))
+        triples = sieve_triples(ntr * (args.steps + args.warmup))
         for w in range(args.warmup):
             sv.run(triples[w * ntr:(w + 1) * ntr], K, dmask, stream=stream.cuda_stream)
         stream.synchronize()
@@ -337,7 +306,7 @@ def main():
     dropin_s = (time.perf_counter() - t0) / 3
 
     # --- Miller-Rabin: resident batch ---------------------------------------
-    pairs = config3_pairs(survivors)
+    pairs = uniform_batch_pairs(survivors)
     cands = [pfb200.build_candidate(*abc1, k, j, rev) for (k, j) in pairs for rev in (False, True)]
     sq_per_test = statistics.mean([(N - 1).bit_length() for N in cands])  # bits(d) + 1 check, s = 1
     eng = pfb200.MillerRabin(dev)
@@ -386,6 +355,35 @@ def main():
     plain_tests_s = plain_sq_s / sq_per_test
     one.close()
 
+    # uneven batch: 512 candidates of 50 000 - 100 000 digits resident at once,
+    # every length advanced by the same persistent launches
+    uneven = None
+    if not args.no_uneven:
+        tup = uneven_tuples(512)
+        ucands = [pfb200.build_candidate(*t) for t in tup]
+        ub = pfb200.MRBatch(eng, ucands, 2)
+        with torch.cuda.stream(stream):
+            ub.advance(64, stream.cuda_stream)
+            stream.synchronize()
+            barrier()
+            d0 = pfb200.batch_steps_done(ub)
+            flush.fill_(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ub.advance(256, stream.cuda_stream)
+            e1.record(stream)
+            stream.synchronize()
+            d1 = pfb200.batch_steps_done(ub)
+        ub.close()
+        t_u = max_over_ranks(e0.elapsed_time(e1) / 1e3)
+        mean_bits = statistics.mean(N.bit_length() for N in ucands)
+        uneven = {"value": (d1 - d0) / t_u / mean_bits * world, "unit": "tests/s",
+                  "candidates": len(ucands), "mean_bits": mean_bits,
+                  "digits": [min(t[0] for t in tup), max(t[0] for t in tup)],
+                  "squarings_per_s": (d1 - d0) / t_u, "ms_per_step": 1e3 * t_u,
+                  "workload": "512 tuples, splitmix64 seed 2: a ~ U[50000,100000], c ~ U[100,1000], "
+                              "b ~ U[c+1,a-1], k,j ~ U[1,9999], N or rev(N); 256 squarings each per step"}
+
     # roofline of the squaring kernel
     peak_lo, peak_hi = pfb200.measure_int32_peak(dev)
     digits = len(str(cands[0]))
@@ -405,17 +403,27 @@ def main():
         # requests: N and rev(N) as separate requests, a ~ U[50000, 100000], c ~ U[100, 1000],
         # b ~ U[c+1, a-1] (redrawn while a-b-lk < 2 or b-c <= lj), k, j ~ U[1, 9999]
         def draw():
-            while True:
-                a = rng.randint(50000, 100000)
-                c = rng.randint(100, 1000)
-                b = rng.randint(c + 1, a - 1)
-                k, j = rng.randint(1, 9999), rng.randint(1, 9999)
-                if a - b - len(str(k)) >= 2 and b - c > len(str(j)):
-                    return pfb200.build_candidate(a, b, c, k, j, bool(rng.getrandbits(1)))
+            return pfb200.build_candidate(*serving_draw(rng))
         props = torch.cuda.get_device_properties(dev)
-        cap_tests_s = squarings / t_mr / (2.25 * sq_per_test * 2.5)  # mean size ~75k digits: ~2.25x bits, ~2.5x time/step
+        resident = 2 * props.multi_processor_count
+        # served capacity on this request mix: a resident batch of `resident` draws,
+        # squarings/s over its mean exponent length
+        mix = [draw() for _ in range(resident)]
+        mb = pfb200.MRBatch(eng, mix, 2)
+        with torch.cuda.stream(stream):
+            mb.advance(128, stream.cuda_stream)
+            stream.synchronize()
+            d0 = pfb200.batch_steps_done(mb)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mb.advance(512, stream.cuda_stream)
+            e1.record(stream)
+            stream.synchronize()
+            d1 = pfb200.batch_steps_done(mb)
+        mb.close()
+        cap_tests_s = (d1 - d0) / (e0.elapsed_time(e1) / 1e3) / statistics.mean(N.bit_length() for N in mix)
         rate = args.serve_load * cap_tests_s
-        srv = pfb200.MRServer(eng, max_resident=2 * props.multi_processor_count, chunk_steps=256)
+        srv = pfb200.MRServer(eng, max_resident=resident, hbm_budget_bytes=150 * 10**9, chunk_steps=256)
         t_start = time.perf_counter()
         next_t, tag, lat, pending = 0.0, 0, [], 0
         while time.perf_counter() - t_start < args.serve_secs:
@@ -434,6 +442,7 @@ def main():
                    "completed": len(lat), "tests_per_s": len(lat) / args.serve_secs,
                    "p50_s": pct(0.50), "p99_s": pct(0.99), "resident_at_end": st["resident"],
                    "queued_at_end": st["queued"], "launches": st["launches"],
+                   "capacity_tests_per_s": cap_tests_s, "max_resident": resident, "hbm_budget_bytes": 150 * 10**9,
                    "workload": "Poisson arrivals (seed 3) of N / rev(N), a ~ U[50000,100000], "
                                "k,j ~ U[1,9999], at %.2fx the estimated capacity" % args.serve_load}
 
@@ -471,6 +480,7 @@ def main():
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
         "plain": {"value": plain_tests_s, "unit": "tests/s", "form": "one candidate per call"},
         "served_over_plain": tests_s / world / plain_tests_s,
+        "uneven": uneven,
         "sieve": {"value": sieve_pairs_s, "unit": "pairs/s", "K": K, "triples_per_step": ntr,
                   "dropin_100x100_s": dropin_s, "dropin_timing": {"upload": t.upload, "kernel": t.kernel,
                                                                   "download": t.download}},

@@ -10,10 +10,12 @@ oracle/mr_oracle.c), the base-2 strong-test residue r = 2^d mod N
                    miller_rabin_test verdicts are stored beside them)
   mr_config3.json  N and rev(N) of every survivor (k,j <= 99) of that sieve:
                    the candidates the 256-number uniform batch draws from
+  mr_config4.json  the first 32 of the 512 uneven-batch tuples
+                   (pfb200.workloads.uneven_tuples: 50 000 - 100 000 digits)
 
 Each 50 000-digit powm takes minutes of one core; the script runs a process
 pool (spawn) over all cores.  Usage:
-  python tests/golden/make_mr_golden.py config1|config3
+  python tests/golden/make_mr_golden.py config1|config3|config4
 """
 import hashlib
 import json
@@ -25,6 +27,7 @@ import time
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
+sys.path.insert(0, os.path.join(ROOT, "prime-finder_b200"))
 
 
 def residue_record(args):
@@ -51,11 +54,15 @@ def main():
     if which == "config1":
         pairs = pairs[:16]
     jobs = [(a, b, c, k, j, rev) for (k, j) in pairs for rev in (False, True)]
+    if which == "config4":
+        from pfb200.workloads import uneven_tuples
+        jobs = uneven_tuples(512)[:32]
     ctx = mp.get_context("spawn")
     with ctx.Pool(os.cpu_count()) as pool:
         recs = pool.map(residue_record, jobs, chunksize=1)
-    out = {"source": "GMP 6.3 mpz_powm via oracle/mr_oracle.c", "base": 2, "abc": [a, b, c],
-           "records": recs}
+    out = {"source": "GMP 6.3 mpz_powm via oracle/mr_oracle.c", "base": 2, "records": recs}
+    if which != "config4":
+        out["abc"] = [a, b, c]
     if which == "config1":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle

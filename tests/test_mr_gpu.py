@@ -195,3 +195,32 @@ def test_resident_batch_stepwise_equals_one_shot(mr):
     v, r = b.results(residues=True)
     assert v == want_v and r == want_r
     b.close()
+
+
+def _check_records(mr, recs):
+    Ns = [oracle.build_candidate(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs]
+    ver, res = mr.test(Ns, 2)
+    for r, N, v, x in zip(recs, Ns, ver, res):
+        n16 = (N.bit_length() + 15) // 16
+        assert N.bit_length() == r["bits"]
+        assert "%016x" % (x & (2**64 - 1)) == r["low64"], (r["a"], r["k"], r["j"], r["rev"])
+        assert hashlib.sha256(x.to_bytes(2 * n16, "little")).hexdigest() == r["sha256"]
+        assert v == r["sprp2"]
+
+
+def test_uniform_batch_every_candidate_residue(mr):
+    """Every number the 256-candidate 50 000-digit batch draws from (N and
+    rev(N) of all 107 survivors): residues hash to GMP's, verdicts match."""
+    g = _golden("mr_config3.json")
+    assert len(g["records"]) == 214
+    _check_records(mr, g["records"])
+
+
+def test_uneven_batch_subset_residues(mr):
+    """The first 32 uneven-batch candidates (50 000 - 100 000 digits, both
+    transform lengths in one batch) against GMP."""
+    from pfb200.workloads import uneven_tuples
+    g = _golden("mr_config4.json")
+    recs = g["records"]
+    assert [(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs] == uneven_tuples(512)[:32]
+    _check_records(mr, recs)
