@@ -40,6 +40,7 @@ sys.set_int_max_str_digits(0)
 from pfb200.workloads import serving_draw, sieve_triples, uneven_tuples, uniform_batch_pairs  # noqa: E402
 
 SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference count)
+PERSIST_LAUNCH_DRAM_BYTES = 137718528 + 21966848  # dram__bytes_read.sum + dram__bytes_write.sum
 
 
 def ref_modmuls_per_squaring(digits: int) -> int:
@@ -390,7 +391,11 @@ def main():
     ref_mults = ref_modmuls_per_squaring(digits) * SQ_PER_MODMUL
     achieved = squarings / t_mr * ref_mults  # INT32 multiplies / s (one GPU)
     roofline = {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_lo / 1e12, "unit": "Tmul/s",
-                "frac": achieved / peak_lo, "traffic": None,
+                "frac": achieved / peak_lo,
+                # DRAM bytes (read + write) of one timed launch of this workload (1024 squarings x
+                # 256 candidates, L2 flushed before it), from one ncu capture of the same command:
+                # profiles/persist_kernel_uniform_batch_dram.txt
+                "traffic": PERSIST_LAUNCH_DRAM_BYTES if chunk == 1024 and n == 256 else None,
                 "peak_source": "measured live: pfb_measure_int32_peak (mul.lo)",
                 "mul_hi_peak": peak_hi / 1e12,
                 "work": "%d INT32 multiplies per squaring (reference structure at %d digits)" % (ref_mults, digits)}

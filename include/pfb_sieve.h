@@ -82,9 +82,10 @@ int pfb_sieve_survivors(pfb_sieve_t *s, const uint8_t *d_mask, int K,
 
 /*
  * Stateless convenience (the shape sketched for trial_div_gpu_grid): host
- * primes, host mask, synchronous, on the current device.  Keeps an internal
- * context per device for the last prime list seen (re-uploaded when the
- * pointer, count or first/last prime changes).
+ * primes, host mask, synchronous, on the current device.  Keeps one internal
+ * context per device and uploads the given prime list into it on every call
+ * (as trial_div_gpu does); callers that sieve many batches with one list
+ * should hold a pfb_sieve_t instead.
  */
 int trial_div_gpu_grid(const uint32_t *primes, uint32_t n_primes,
                        const long long *abc, int n_abc, int K, uint8_t *mask_out,
