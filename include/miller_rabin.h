@@ -6,10 +6,10 @@
  * - rev(j)*10^(a-c-lj) - 1 (miller_rabin.c:56-99).  Returns 0 when N is
  * composite (rev(N) not tested), 1 when N is a probable prime and rev(N)
  * composite, 2 when both are probable primes; -1 on bad arguments or a GPU
- * failure.  The reference calls GMP's mpz_probab_prime_p(x, 5) (BPSW); this
- * one runs strong probable-prime rounds to the bases 2, 3, 5, 7 and 11 on the
- * GPU, stopping at the first failed round.  The two agree on every composite
- * that is not a strong pseudoprime to all five bases at once.
+ * failure.  The reference calls GMP's mpz_probab_prime_p(x, 5), which in GMP
+ * 6.2+ is the Baillie-PSW test; this one runs the same test on the GPU (the
+ * strong test to base 2, then the strong Lucas test with Selfridge's
+ * parameters: pfb_mr_bpsw), so the verdicts are the same.
  */
 #pragma once
 

@@ -40,6 +40,8 @@ typedef struct {
 /* Engine on `device`: twiddle tables and constants are set up once. */
 int pfb_mr_create(pfb_mr_t **out, int device);
 void pfb_mr_destroy(pfb_mr_t *e);
+/* Device the engine was created on, or -1 for NULL. */
+int pfb_mr_device(const pfb_mr_t *e);
 
 /*
  * Strong probable-prime test (one Miller-Rabin round) to base `base` for n
@@ -54,6 +56,26 @@ void pfb_mr_destroy(pfb_mr_t *e);
  */
 int pfb_mr_test(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,
                 int8_t *verdict, uint16_t *residue, int residue_stride);
+
+/*
+ * Strong Lucas probable-prime test with Selfridge's parameters (method A: D
+ * the first of 5, -7, 9, -11, ... with Jacobi (D/N) = -1, P = 1,
+ * Q = (1 - D)/4): the second half of the Baillie-PSW test that GMP's
+ * mpz_probab_prime_p runs for the reference's miller_rabin_test
+ * (miller_rabin.c:95,107).  With N + 1 = 2^s d (d odd), N passes when
+ * U_d == 0 or V_(d 2^r) == 0 (mod N) for some r < s.  verdict[i]: 1 strong
+ * Lucas probable prime, 0 composite (a perfect square, or gcd(|D|, N) a proper
+ * factor), -1 invalid (even, below 3, or too long for the ladder's headroom).
+ */
+int pfb_mr_lucas(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, int8_t *verdict);
+
+/*
+ * Baillie-PSW: the strong test to base 2, then pfb_mr_lucas on the numbers
+ * that pass -- the decision GMP 6.2+ makes in mpz_probab_prime_p(N, reps) for
+ * reps <= 24 (the reference calls it with reps = 5).  verdict[i]: 1 probable
+ * prime, 0 composite (also even N > 2 and N < 2), -1 too long.
+ */
+int pfb_mr_bpsw(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, int8_t *verdict);
 
 /*
  * Modular power with a small base: residue_i = base^exp_i mod N_i (the

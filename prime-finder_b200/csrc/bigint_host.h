@@ -155,42 +155,58 @@ inline Words neg_inv_pow2(const Words &N, size_t bits) {
     return r;
 }
 
-// 2^e mod N by Knuth's algorithm D on 32-bit digits (N > 1).
-inline Words pow2_mod(size_t e, const Words &N) {
-    // digits of N
-    std::vector<uint32_t> v;
-    for (uint64_t w : N) {
-        v.push_back((uint32_t)w);
-        v.push_back((uint32_t)(w >> 32));
-    }
-    while (!v.empty() && v.back() == 0) v.pop_back();
+// Quotient and remainder of U / V (V > 0) by Knuth's algorithm D on 32-bit
+// digits (TAOCP vol. 2, 4.3.1).
+inline void divmod(const Words &U, const Words &V, Words *quot, Words *rem) {
+    auto digits = [](const Words &a) {
+        std::vector<uint32_t> d;
+        for (uint64_t w : a) {
+            d.push_back((uint32_t)w);
+            d.push_back((uint32_t)(w >> 32));
+        }
+        while (!d.empty() && d.back() == 0) d.pop_back();
+        return d;
+    };
+    auto words = [](const std::vector<uint32_t> &d) {
+        Words w((d.size() + 1) / 2, 0);
+        for (size_t i = 0; i < d.size(); i++) w[i / 2] |= (uint64_t)d[i] << (32 * (i % 2));
+        trim(w);
+        return w;
+    };
+    const std::vector<uint32_t> v = digits(V), u = digits(U);
     const size_t n = v.size();
-    // u = 2^e as digits
-    std::vector<uint32_t> u(e / 32 + 1, 0);
-    u[e / 32] = 1u << (e % 32);
+    if (u.size() < n || cmp(U, V) < 0) {
+        if (quot) *quot = Words();
+        if (rem) {
+            *rem = U;
+            trim(*rem);
+        }
+        return;
+    }
+    const size_t m = u.size() - n;
+    std::vector<uint32_t> q(m + 1, 0);
     if (n == 1) {
         uint64_t r = 0;
-        for (size_t i = u.size(); i-- > 0;) r = ((r << 32) | u[i]) % v[0];
-        return Words(1, r);
-    }
-    if (u.size() < n) {  // 2^e < N
-        Words r((u.size() + 1) / 2, 0);
-        for (size_t i = 0; i < u.size(); i++) r[i / 2] |= (uint64_t)u[i] << (32 * (i % 2));
-        trim(r);
-        return r;
+        for (size_t i = u.size(); i-- > 0;) {
+            const uint64_t cur = (r << 32) | u[i];
+            if (i <= m) q[i] = (uint32_t)(cur / v[0]);
+            r = cur % v[0];
+        }
+        if (quot) *quot = words(q);
+        if (rem) *rem = r ? Words(1, r) : Words();
+        return;
     }
     const int s = __builtin_clz(v[n - 1]);
     std::vector<uint32_t> vn(n), un(u.size() + 1);
     for (size_t i = n - 1; i > 0; i--) vn[i] = (v[i] << s) | (s ? (uint32_t)((uint64_t)v[i - 1] >> (32 - s)) : 0u);
     vn[0] = v[0] << s;
-    const size_t m = u.size() - n;
     un[u.size()] = s ? (uint32_t)((uint64_t)u[u.size() - 1] >> (32 - s)) : 0u;
     for (size_t i = u.size() - 1; i > 0; i--) un[i] = (u[i] << s) | (s ? (uint32_t)((uint64_t)u[i - 1] >> (32 - s)) : 0u);
     un[0] = u[0] << s;
     const uint64_t b = 1ull << 32;
     for (size_t jj = m + 1; jj-- > 0;) {
         const size_t j = jj;
-        uint64_t num = ((uint64_t)un[j + n] << 32) | un[j + n - 1];
+        const uint64_t num = ((uint64_t)un[j + n] << 32) | un[j + n - 1];
         uint64_t qhat = num / vn[n - 1];
         uint64_t rhat = num - qhat * vn[n - 1];
         while (qhat >= b || qhat * vn[n - 2] > ((rhat << 32) | un[j + n - 2])) {
@@ -210,6 +226,7 @@ inline Words pow2_mod(size_t e, const Words &N) {
         const int64_t t = (int64_t)un[j + n] - (int64_t)carry - borrow;
         un[j + n] = (uint32_t)t;
         if (t < 0) {  // add back
+            qhat--;
             uint64_t c = 0;
             for (size_t i = 0; i < n; i++) {
                 const uint64_t sum = (uint64_t)un[i + j] + vn[i] + c;
@@ -218,15 +235,31 @@ inline Words pow2_mod(size_t e, const Words &N) {
             }
             un[j + n] += (uint32_t)c;
         }
+        q[j] = (uint32_t)qhat;
     }
-    // remainder = un[0..n) >> s
-    std::vector<uint32_t> r(n);
-    for (size_t i = 0; i < n; i++)
-        r[i] = (un[i] >> s) | (s ? (uint32_t)((uint64_t)un[i + 1] << (32 - s)) : 0u);
-    Words out((n + 1) / 2, 0);
-    for (size_t i = 0; i < n; i++) out[i / 2] |= (uint64_t)r[i] << (32 * (i % 2));
-    trim(out);
-    return out;
+    if (quot) *quot = words(q);
+    if (rem) {
+        std::vector<uint32_t> r(n);
+        for (size_t i = 0; i < n; i++)
+            r[i] = (un[i] >> s) | (s ? (uint32_t)((uint64_t)un[i + 1] << (32 - s)) : 0u);
+        *rem = words(r);
+    }
+}
+
+// 2^e mod N (N > 1).
+inline Words pow2_mod(size_t e, const Words &N) {
+    Words u(e / 64 + 1, 0);
+    u[e / 64] = 1ull << (e % 64);
+    Words r;
+    divmod(u, N, nullptr, &r);
+    return r;
+}
+
+// a mod m for 0 < m < 2^32.
+inline uint32_t mod_small(const Words &a, uint32_t m) {
+    unsigned __int128 r = 0;
+    for (size_t i = a.size(); i-- > 0;) r = ((r << 64) | a[i]) % m;
+    return (uint32_t)r;
 }
 
 // a * b, schoolbook.
@@ -284,6 +317,29 @@ inline Words sub(const Words &a, const Words &b) {
     }
     trim(r);
     return r;
+}
+
+// floor(sqrt(a)) by Newton's iteration from a power of two above the root.
+inline Words isqrt(const Words &a) {
+    const size_t bits = bit_length(a);
+    if (bits == 0) return Words();
+    Words x = shl(Words(1, 1), (bits + 1) / 2);
+    for (;;) {
+        Words q;
+        divmod(a, x, &q, nullptr);
+        // y = (x + a / x) / 2
+        Words y(std::max(x.size(), q.size()) + 1, 0);
+        unsigned __int128 c = 0;
+        for (size_t i = 0; i < y.size(); i++) {
+            c += (unsigned __int128)(i < x.size() ? x[i] : 0) + (i < q.size() ? q[i] : 0);
+            y[i] = (uint64_t)c;
+            c >>= 64;
+        }
+        trim(y);
+        y = shr(y, 1);
+        if (cmp(y, x) >= 0) return x;
+        x = y;
+    }
 }
 
 // 10^e = 5^e * 2^e (square-and-multiply on 5^e).

@@ -34,14 +34,23 @@ struct JobDev {
     uint32_t *spill_s;    // L words  (sequential-prime step only)
     uint32_t *spill_t;    // H words  (sequential-prime step only)
     uint32_t *ybuf;       // H words  (sequential-prime step only: canonical residue)
+    struct LucasDev *lucas;  // strong Lucas test (mode 2) only
     int logl;
     int cursor;   // next exponent bit (MSB first); phase 0 while >= 0
     int extra;    // squarings left in phase 2 (s - 1 for a strong test)
     int phase;    // 0 exponent loop, 1 first check, 2 squarings r < s, 3 done
     uint32_t base;
-    int mode;     // 0 modular power only, 1 strong test
+    int mode;     // 0 modular power only, 1 strong test, 2 strong Lucas test
     int verdict;  // 1 probable prime, 0 composite
     int steps;    // steps taken (diagnostics)
+};
+
+// Strong Lucas state of one candidate: H limbs each, Montgomery form: V_k,
+// V_(k+1), Q^k, a product, R mod N; gy the [2][L] spectrum of V_(k+1).
+struct LucasDev {
+    uint32_t *lv0, *lv1, *lqk, *lt, *lone, *gy;
+    int q;        // Selfridge Q = (1 - D) / 4
+    uint32_t lb;  // every stored value is < lb * N
 };
 
 // Shared memory: both primes' transforms + X + Y up to L = 2^LOG_LCTA; one
@@ -122,18 +131,34 @@ __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, const in
     }
 }
 
-// One Montgomery step in the layout chosen by the transform length.
-__device__ __forceinline__ void mstep(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                                      const JobDev &jb) {
+// One Montgomery step in the layout chosen by the transform length (gy: the
+// spectrum of a second factor, see mont_step).
+template <bool MUL>
+__device__ __forceinline__ void mstep_t(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
+                                        const JobDev &jb, const uint32_t *gy) {
     if (cd.logl <= LOG_LCTA) {
-        mont_step(sm, cd, square, a, tw, c_crt);
+        mont_step<MUL>(sm, cd, square, a, tw, c_crt, gy);
     } else {
         const Spill sp{jb.spill_s, jb.spill_t};
-        mont_step_seq(sm, cd, square, a, tw, c_crt, sp);
+        mont_step_seq<MUL>(sm, cd, square, a, tw, c_crt, sp, gy);
     }
 }
 
+// The strong test's squarings (inlined into its loop).
+__device__ __forceinline__ void mstep(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
+                                      const JobDev &jb) {
+    mstep_t<false>(sm, cd, square, a, tw, jb, nullptr);
+}
+
+// The Lucas ladder's steps: one out-of-line copy with the general product, so
+// the strong test's loop keeps its own register allocation.
+__device__ __noinline__ void mstep_l(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
+                                     const JobDev &jb, const uint32_t *gy) {
+    mstep_t<true>(sm, cd, square, a, tw, jb, gy);
+}
+
 // Canonical residue of X (Montgomery form) into Y: Y = X R^-1 mod N.
+template <bool LUCAS = false>
 __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uint32_t *nl, const Twiddles &tw,
                           const JobDev &jb) {
     const int H = 1 << (cd.logl - 1);
@@ -141,7 +166,8 @@ __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uin
     __syncthreads();
     Smem s2 = sm;
     s2.X = Y;
-    mstep(s2, cd, false, 1u, tw, jb);
+    if (LUCAS) mstep_l(s2, cd, false, 1u, tw, jb, nullptr);
+    else mstep(s2, cd, false, 1u, tw, jb);
     // REDC(X) lies in [0, N]; it is N only when X == 0 (mod N), e.g. a base
     // that is a multiple of N.  Map it to 0.
     bool eqn = true;
@@ -149,6 +175,179 @@ __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uin
     if (__syncthreads_and(eqn))
         for (int i = threadIdx.x; i < H; i += blockDim.x) Y[pad(i)] = 0u;
     __syncthreads();
+}
+
+// ------------------------------------------------------- strong Lucas ----
+// Selfridge's method A (P = 1, Q = (1 - D)/4) on the squaring engine.  With
+// N + 1 = 2^s d, d odd, N is a strong Lucas probable prime when U_d == 0 or
+// V_(d 2^r) == 0 (mod N) for some 0 <= r < s.  The ladder keeps (V_k,
+// V_(k+1), Q^k) and for each bit b of d, from the top, moves k to 2k + b:
+//   V_2k = V_k^2 - 2 Q^k,  V_2k+1 = V_k V_(k+1) - Q^k,  V_2k+2 = V_(k+1)^2 - 2 Q^(k+1),
+// Q^2k = (Q^k)^2, Q^(2k+1) = Q (Q^k)^2.  Since D U_k = 2 V_(k+1) - V_k and
+// gcd(D, N) = 1, U_d == 0 is tested as V_d - 2 V_(d+1) == 0.
+// Values are kept below lb N (lb = 2 + 4 Q^2) and R > lb^2 N keeps every
+// product's REDC below 2N.
+
+__device__ __forceinline__ void load_res(uint32_t *X, const uint32_t *src, int H) {
+    for (int i = threadIdx.x; i < H; i += blockDim.x) X[pad(i)] = __ldcg(src + i);
+    __syncthreads();
+}
+
+__device__ __forceinline__ void store_res(uint32_t *dst, const uint32_t *X, int H) {
+    for (int i = threadIdx.x; i < H; i += blockDim.x) dst[i] = X[pad(i)];
+    __syncthreads();
+}
+
+// g[2][L] <- NTT_L of the H limbs at src (zero-padded), both primes, reduced.
+__device__ void spectrum(const Smem &sm, int logl, const uint32_t *src, uint32_t *g, const Twiddles &tw) {
+    const int L = 1 << logl, H = L >> 1;
+    if (logl <= LOG_LCTA) {
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            const uint32_t v = i < H ? __ldcg(src + i) : 0u;
+            sm.A0[pad(i)] = v;
+            sm.A1[pad(i)] = v;
+        }
+        __syncthreads();
+        dif(sm.A0, sm.A1, logl, tw);
+        for (int i = threadIdx.x; i < L; i += blockDim.x) {
+            g[i] = red2(sm.A0[pad(i)], P1);
+            g[L + i] = red2(sm.A1[pad(i)], P2);
+        }
+        __syncthreads();
+        return;
+    }
+    uint32_t *A = sm.A0;
+    for (int pr = 0; pr < 2; pr++) {
+        for (int i = threadIdx.x; i < L; i += blockDim.x) A[pad(i)] = i < H ? __ldcg(src + i) : 0u;
+        __syncthreads();
+        if (pr == 0) dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
+        else dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
+        const uint32_t p = pr ? P2 : P1;
+        for (int i = threadIdx.x; i < L; i += blockDim.x) g[pr * L + i] = red2(A[pad(i)], p);
+        __syncthreads();
+    }
+}
+
+// out <- x + c y (sub = false) or x + c (m N - y) (sub = true: x - c y mod N,
+// for y < m N), over H limbs; x(i) and y(i) read limb i of the operands
+// (x may return 0).  m N - y is formed as m N + (B^H - 1 - y) + 1 - B^H so
+// every coefficient is non-negative; the B^H term is the carry out of the
+// top limb, dropped (the result itself is below R = B^H).
+template <bool OPAD, class GX, class GY>
+__device__ void lincomb(uint32_t *out, GX x, GY y, const uint32_t *nl, uint32_t c, uint32_t m, bool sub, int H,
+                        CarrySmem &cs) {
+    const unsigned long long cm = (unsigned long long)c * m;
+    if (sub)
+        carry_pass<OPAD>(H, 0ull, [&](int i) {
+            return x(i) + cm * __ldg(nl + i) + (unsigned long long)c * (LIMB_MASK - y(i)) + (i == 0 ? c : 0u);
+        }, out, cs);
+    else
+        carry_pass<OPAD>(H, 0ull, [&](int i) { return x(i) + (unsigned long long)c * y(i); }, out, cs);
+}
+
+// Is the value in X zero mod N?  (Y receives its canonical residue.)
+__device__ bool residue_zero(const Smem &sm, uint32_t *Y, const Cand &cd, const JobDev &jb, const Twiddles &tw) {
+    canonical<true>(sm, Y, cd, jb.nl, tw, jb);
+    const int H = 1 << (cd.logl - 1);
+    bool z = true;
+    for (int i = threadIdx.x; i < H; i += blockDim.x) z = z && (Y[pad(i)] == 0u);
+    return __syncthreads_and(z) != 0;
+}
+
+// One ladder bit: (V_k, V_(k+1), Q^k) -> k' = 2k + bit.
+__device__ void lucas_bit(const Smem &sm, const Cand &cd, const JobDev &jb, const LucasDev &lc, uint32_t bit,
+                          const Twiddles &tw) {
+    const int H = 1 << (cd.logl - 1);
+    CarrySmem &cs = *sm.cs;
+    const uint32_t aq = (uint32_t)(lc.q < 0 ? -lc.q : lc.q), mq = 2u * aq;  // Q^k < 2|Q| N
+    uint32_t *X = sm.X;
+    auto gX = [&](int i) { return (unsigned long long)X[pad(i)]; };
+    auto g0 = [&](int) { return 0ull; };
+    auto glt = [&](int i) { return (unsigned long long)__ldcg(lc.lt + i); };
+    auto gqk = [&](int i) { return (unsigned long long)__ldcg(lc.lqk + i); };
+    // T1 = V_k V_(k+1) -> lt
+    spectrum(sm, cd.logl, lc.lv1, lc.gy, tw);
+    load_res(X, lc.lv0, H);
+    mstep_l(sm, cd, false, 1u, tw, jb, lc.gy);
+    store_res(lc.lt, X, H);
+    // T2 = V_k^2 (bit 0) or V_(k+1)^2 (bit 1), in X
+    load_res(X, bit ? lc.lv1 : lc.lv0, H);
+    mstep_l(sm, cd, true, 1u, tw, jb, nullptr);
+    if (!bit) {
+        lincomb<false>(lc.lv0, gX, gqk, jb.nl, 2u, mq, true, H, cs);   // V_2k   = T2 - 2 Q^k
+        lincomb<false>(lc.lv1, glt, gqk, jb.nl, 1u, mq, true, H, cs);  // V_2k+1 = T1 - Q^k
+    } else {
+        lincomb<false>(lc.lv0, glt, gqk, jb.nl, 1u, mq, true, H, cs);  // V_2k+1 = T1 - Q^k
+        // V_2k+2 = T2 - 2 Q Q^k
+        lincomb<false>(lc.lv1, gX, gqk, jb.nl, 2u * aq, mq, lc.q > 0, H, cs);
+    }
+    if (aq == 1u) {  // Q = -1: Q^k' = (-1)^k' = (-1)^bit
+        auto gone = [&](int i) { return (unsigned long long)__ldcg(lc.lone + i); };
+        lincomb<false>(lc.lqk, g0, gone, jb.nl, 1u, 2u, bit != 0u, H, cs);
+    } else {
+        load_res(X, lc.lqk, H);
+        mstep_l(sm, cd, true, bit ? aq : 1u, tw, jb, nullptr);  // (Q^k)^2 |Q|^bit < 2 |Q| N
+        lincomb<false>(lc.lqk, g0, gX, jb.nl, 1u, mq, bit && lc.q < 0, H, cs);
+    }
+}
+
+// Strong Lucas steps of one candidate (mode 2); returns steps taken.
+__device__ __noinline__ int run_lucas(JobDev &jb, const Smem &sm, uint32_t *Y, int max_steps, const Twiddles &tw, int &cursor,
+                         int &phase, int &extra, int &verdict) {
+    const Cand cd{jb.nph, jb.nh, jb.logl};
+    const LucasDev lc = *jb.lucas;
+    const int H = 1 << (jb.logl - 1);
+    CarrySmem &cs = *sm.cs;
+    const uint32_t aq = (uint32_t)(lc.q < 0 ? -lc.q : lc.q), mq = 2u * aq;
+    auto g0 = [&](int) { return 0ull; };
+    auto gqk = [&](int i) { return (unsigned long long)__ldcg(lc.lqk + i); };
+    auto gX = [&](int i) { return (unsigned long long)sm.X[pad(i)]; };
+    int steps = 0;
+    while (steps < max_steps && phase != 3) {
+        if (phase == 0) {
+            const uint32_t bit = (__ldg(jb.exp + (cursor >> 5)) >> (cursor & 31)) & 1u;
+            lucas_bit(sm, cd, jb, lc, bit, tw);
+            cursor--;
+            if (cursor < 0) phase = 1;
+        } else {
+            if (phase == 2) {  // V_2m = V_m^2 - 2 Q^m, Q^2m = (Q^m)^2
+                load_res(sm.X, lc.lv0, H);
+                mstep_l(sm, cd, true, 1u, tw, jb, nullptr);
+                lincomb<false>(lc.lv0, gX, gqk, jb.nl, 2u, mq, true, H, cs);
+                if (aq == 1u) {  // Q^2m = 1
+                    auto gone = [&](int i) { return (unsigned long long)__ldcg(lc.lone + i); };
+                    lincomb<false>(lc.lqk, g0, gone, jb.nl, 1u, 2u, false, H, cs);
+                } else {
+                    load_res(sm.X, lc.lqk, H);
+                    mstep_l(sm, cd, true, 1u, tw, jb, nullptr);
+                    store_res(lc.lqk, sm.X, H);
+                }
+                extra--;
+            }
+            bool hit = false;
+            if (phase == 1) {  // U_d == 0  <=>  V_d - 2 V_(d+1) == 0
+                auto gv0 = [&](int i) { return (unsigned long long)__ldcg(lc.lv0 + i); };
+                auto gv1 = [&](int i) { return (unsigned long long)__ldcg(lc.lv1 + i); };
+                lincomb<true>(sm.X, gv0, gv1, jb.nl, 2u, lc.lb, true, H, cs);
+                hit = residue_zero(sm, Y, cd, jb, tw);
+            }
+            if (!hit) {  // V_(d 2^r) == 0
+                load_res(sm.X, lc.lv0, H);
+                hit = residue_zero(sm, Y, cd, jb, tw);
+            }
+            if (hit) {
+                verdict = 1;
+                phase = 3;
+            } else if (extra <= 0) {
+                verdict = 0;
+                phase = 3;
+            } else {
+                phase = 2;
+            }
+        }
+        steps++;
+    }
+    return steps;
 }
 
 // Runs up to max_steps steps of one candidate.  The job's state is read with
@@ -168,10 +367,22 @@ __device__ void run_job(JobDev *jp, int max_steps, const Twiddles &tw, uint32_t 
     carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int H = 1 << (jb.logl - 1);
     const Cand cd{jb.nph, jb.nh, jb.logl};
+    int cursor = jb.cursor, phase = jb.phase, extra = jb.extra, verdict = jb.verdict, steps = 0;
+    if (jb.mode == 2) {
+        steps = run_lucas(jb, sm, Y, max_steps, tw, cursor, phase, extra, verdict);
+        if (threadIdx.x == 0) {
+            jp->cursor = cursor;
+            jp->phase = phase;
+            jp->extra = extra;
+            jp->verdict = verdict;
+            jp->steps = jb.steps + steps;
+        }
+        __syncthreads();
+        return;
+    }
     for (int i = threadIdx.x; i < H; i += blockDim.x) sm.X[pad(i)] = __ldcg(jb.x + i);
     __syncthreads();
 
-    int cursor = jb.cursor, phase = jb.phase, extra = jb.extra, verdict = jb.verdict, steps = 0;
     while (steps < max_steps && phase != 3) {
         if (phase == 0) {
             const uint32_t bit = (__ldg(jb.exp + (cursor >> 5)) >> (cursor & 31)) & 1u;
@@ -276,12 +487,16 @@ static uint32_t powmod_h(uint64_t b, uint64_t e, uint32_t p) {
 static uint32_t shoup_c(uint32_t w, uint32_t p) { return (uint32_t)(((uint64_t)w << 32) / p); }
 
 struct HostPrep {
-    int ok = 0;  // 1 = valid
+    int ok = 0;        // 1 = valid
+    int decided = -1;  // >= 0: verdict known without device work (Lucas: a factor, a square)
     int logl = 0;
     int s = 0;
     std::vector<uint32_t> x0, npl, nl, exp;
     int cursor = 0;
     int n16 = 0;  // limbs of N (16-bit)
+    int q = 0;                 // Lucas: Q
+    uint32_t lb = 0;           // Lucas: value bound factor
+    std::vector<uint32_t> v0;  // Lucas: V_0 = 2 in Montgomery form
 };
 
 static int choose_logl(size_t nbits, uint32_t base) {
@@ -293,7 +508,65 @@ static int choose_logl(size_t nbits, uint32_t base) {
     return -1;
 }
 
-// mode 1: exponent d of N - 1 = 2^s d; mode 0: exponent given.
+static uint32_t gcd_u32(uint32_t a, uint32_t b) {
+    while (b) {
+        const uint32_t t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+// Jacobi symbol (a / n), n odd > 0.
+static int jacobi_u32(uint32_t a, uint32_t n) {
+    a %= n;
+    int t = 1;
+    while (a) {
+        while (!(a & 1u)) {
+            a >>= 1;
+            const uint32_t r = n & 7u;
+            if (r == 3u || r == 5u) t = -t;
+        }
+        std::swap(a, n);
+        if ((a & 3u) == 3u && (n & 3u) == 3u) t = -t;
+        a %= n;
+    }
+    return n == 1u ? t : 0;
+}
+
+// Selfridge's method A for odd N > 1: D the first of 5, -7, 9, -11, ... with
+// (D / N) = -1; Q = (1 - D) / 4.  Returns 1 with D set, 0 when N is composite
+// (a factor gcd(|D|, N) < N, or a perfect square), -1 when no D with |D| <=
+// 2001 works (not reached by non-squares in practice).
+static int selfridge(const pfb::big::Words &N, long &D_out) {
+    using namespace pfb::big;
+    const bool small = bit_length(N) <= 32;
+    const int n_mod4 = (int)(N[0] & 3ull);
+    long D = 5;
+    for (int tries = 1;; tries++) {
+        const uint32_t ad = (uint32_t)(D < 0 ? -D : D);
+        const uint32_t r = mod_small(N, ad);
+        const uint32_t g = gcd_u32(ad, r);
+        if (g > 1u && !(small && N[0] == g)) return 0;
+        // (|D| / N) = (N mod |D| / |D|) (-1)^((|D|-1)/2 (N-1)/2); (-1 / N) = (-1)^((N-1)/2)
+        int j = jacobi_u32(r, ad);
+        if ((ad & 3u) == 3u && n_mod4 == 3) j = -j;
+        if (D < 0 && n_mod4 == 3) j = -j;
+        if (j == -1) {
+            D_out = D;
+            return 1;
+        }
+        if (tries == 6) {  // (D / N) = -1 never happens for a square N
+            const Words r2 = isqrt(N);
+            if (cmp(mul(r2, r2), N) == 0) return 0;
+        }
+        D = D > 0 ? -(D + 2) : -D + 2;
+        if ((D < 0 ? -D : D) > 2001) return -1;
+    }
+}
+
+// mode 1: exponent d of N - 1 = 2^s d; mode 0: exponent given; mode 2: the
+// strong Lucas test, exponent d of N + 1 = 2^s d.
 static void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const pfb_mr_number_t *ex,
                       HostPrep &hp) {
     using namespace pfb::big;
@@ -302,6 +575,20 @@ static void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const
     Words N = from_u16(num.limbs, (size_t)num.n_limbs);
     const size_t nb = bit_length(N);
     if (nb < 2 || !(N[0] & 1ull) || nb > (size_t)PFB_MR_MAX_BITS) return;
+    if (mode == 2) {
+        long D = 0;
+        const int sel = selfridge(N, D);
+        if (sel < 0) return;
+        if (sel == 0) {
+            hp.ok = 1;
+            hp.decided = 0;
+            return;
+        }
+        hp.q = (int)((1 - D) / 4);
+        const uint32_t aq = (uint32_t)(hp.q < 0 ? -hp.q : hp.q);
+        hp.lb = 2u + 4u * aq * aq;
+        base = hp.lb;
+    }
     const int lg = choose_logl(nb, base);
     if (lg < 0) return;
     const size_t H = (size_t)1 << (lg - 1);
@@ -312,6 +599,13 @@ static void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const
         Words nm1 = sub_small(N, 1);
         while (!test_bit(nm1, (size_t)s)) s++;
         E = shr(nm1, (size_t)s);
+    } else if (mode == 2) {
+        Words np1 = N;
+        size_t i = 0;
+        while (i < np1.size() && ++np1[i] == 0) i++;
+        if (i == np1.size()) np1.push_back(1);
+        while (!test_bit(np1, (size_t)s)) s++;
+        E = shr(np1, (size_t)s);
     } else {
         if (!ex || !ex->limbs || ex->n_limbs <= 0) return;
         E = from_u16(ex->limbs, (size_t)ex->n_limbs);
@@ -325,7 +619,12 @@ static void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const
     hp.x0.assign(H, 0);
     to_limbs(neg_inv_pow2(N, rbits), LIMB_BITS, hp.npl.data(), H);
     to_limbs(N, LIMB_BITS, hp.nl.data(), H);
-    to_limbs(pow2_mod(rbits, N), LIMB_BITS, hp.x0.data(), H);
+    const Words x0 = pow2_mod(rbits, N);
+    to_limbs(x0, LIMB_BITS, hp.x0.data(), H);
+    if (mode == 2) {
+        hp.v0.assign(H, 0);
+        to_limbs(mul_small(x0, 2), LIMB_BITS, hp.v0.data(), H);
+    }
     const size_t eb = bit_length(E);
     hp.cursor = (int)eb - 1;
     hp.exp.assign((eb + 31) / 32 + 1, 0);
@@ -435,6 +734,8 @@ static int build_tables(pfb_mr *e) {
     return PFB_OK;
 }
 
+extern "C" int pfb_mr_device(const pfb_mr_t *e) { return e ? e->device : -1; }
+
 extern "C" int pfb_mr_create(pfb_mr_t **out, int device) {
     if (!out) {
         pfb::set_error("pfb_mr_create: null out");
@@ -487,10 +788,10 @@ namespace {
 
 // Per-candidate device layout inside the arena (32-bit words).
 struct Layout {
-    size_t x, res, nph, nh, npl, nl, exp, ss, st, yb, total;
+    size_t x, res, nph, nh, npl, nl, exp, ss, st, yb, lv0, lv1, lqk, lt, lone, gy, total;
 };
 
-Layout layout_for(int logl, size_t exp_words) {
+Layout layout_for(int logl, size_t exp_words, bool lucas = false) {
     const size_t L = (size_t)1 << logl, H = L / 2;
     Layout l{};
     size_t o = 0;
@@ -511,11 +812,19 @@ Layout layout_for(int logl, size_t exp_words) {
         l.st = take(H);
         l.yb = take(H + H / 32);  // padded like the shared-memory residue
     }
+    if (lucas) {
+        l.lv0 = take(H);
+        l.lv1 = take(H);
+        l.lqk = take(H);
+        l.lt = take(H);
+        l.lone = take(H);
+        l.gy = take(2 * L);
+    }
     l.total = o;
     return l;
 }
 
-Layout layout_for(const HostPrep &hp) { return layout_for(hp.logl, hp.exp.size()); }
+Layout layout_for(const HostPrep &hp, bool lucas) { return layout_for(hp.logl, hp.exp.size(), lucas); }
 
 // Slot layout of the server: the exponent region sized for the longest
 // modulus of the length class, so that slots of one class are interchangeable.
@@ -552,8 +861,10 @@ struct pfb_mr_batch {
     JobDev *d_jobs = nullptr;
     int *d_locks = nullptr;           // [n] per-candidate locks of the persistent kernel
     unsigned int *d_counter = nullptr;  // quanta handed out in the current launch
+    LucasDev *d_lucas = nullptr;        // [n] (strong Lucas batches only)
     std::vector<HostPrep> hp;
     std::vector<JobDev> jobs;
+    std::vector<LucasDev> lucas;
 };
 
 namespace {
@@ -574,8 +885,8 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     std::vector<Layout> lay(n);
     size_t total = 0;
     for (int i = 0; i < n; i++) {
-        if (!b->hp[i].ok) continue;
-        lay[i] = layout_for(b->hp[i]);
+        if (!b->hp[i].ok || b->hp[i].decided >= 0) continue;
+        lay[i] = layout_for(b->hp[i], mode == 2);
         total += lay[i].total;
         b->maxlog = std::max(b->maxlog, b->hp[i].logl);
         b->max_steps = std::max(b->max_steps, (long long)b->hp[i].cursor + 2 + b->hp[i].s);
@@ -583,7 +894,8 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     }
     const size_t job_bytes = ((size_t)n * sizeof(JobDev) + 255) & ~(size_t)255;
     const size_t lock_bytes = ((size_t)n * sizeof(int) + 256 + 255) & ~(size_t)255;
-    const size_t need = job_bytes + lock_bytes + total * sizeof(uint32_t);
+    const size_t lucas_bytes = mode == 2 ? (((size_t)n * sizeof(LucasDev) + 255) & ~(size_t)255) : 0;
+    const size_t need = job_bytes + lock_bytes + lucas_bytes + total * sizeof(uint32_t);
     if (cudaMalloc(&b->d_arena, need) != cudaSuccess) {
         cudaGetLastError();
         pfb::set_error("pfb_mr: cannot allocate %zu bytes of device memory", need);
@@ -593,7 +905,11 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     b->d_jobs = (JobDev *)b->d_arena;
     b->d_locks = (int *)(b->d_arena + job_bytes);
     b->d_counter = (unsigned int *)(b->d_arena + job_bytes + lock_bytes - 256);
-    uint32_t *d_words = (uint32_t *)(b->d_arena + job_bytes + lock_bytes);
+    if (mode == 2) {
+        b->d_lucas = (LucasDev *)(b->d_arena + job_bytes + lock_bytes);
+        b->lucas.assign(n, LucasDev{});
+    }
+    uint32_t *d_words = (uint32_t *)(b->d_arena + job_bytes + lock_bytes + lucas_bytes);
     if (cudaMemsetAsync(b->d_locks, 0, lock_bytes, e->stream) != cudaSuccess) {
         cudaFree(b->d_arena);
         delete b;
@@ -606,9 +922,9 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
         JobDev &j = b->jobs[i];
         memset(&j, 0, sizeof(j));
         const HostPrep &h = b->hp[i];
-        if (!h.ok) {
+        if (!h.ok || h.decided >= 0) {
             j.phase = 3;
-            j.verdict = -1;
+            j.verdict = h.ok ? h.decided : -1;
             continue;
         }
         uint32_t *w = d_words + off;
@@ -627,12 +943,29 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
         }
         j.logl = h.logl;
         j.cursor = h.cursor;
-        j.extra = mode == 1 ? h.s - 1 : 0;
+        j.extra = mode >= 1 ? h.s - 1 : 0;
         j.phase = 0;
         j.base = base;
         j.mode = mode;
         const size_t H = h.x0.size();
         cudaError_t ce = cudaMemcpyAsync(j.x, h.x0.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+        if (mode == 2) {
+            LucasDev &lc = b->lucas[i];
+            lc.lv0 = w + l.lv0;
+            lc.lv1 = w + l.lv1;
+            lc.lqk = w + l.lqk;
+            lc.lt = w + l.lt;
+            lc.lone = w + l.lone;
+            lc.gy = w + l.gy;
+            lc.q = h.q;
+            lc.lb = h.lb;
+            j.lucas = b->d_lucas + i;
+            // V_0 = 2, V_1 = P = 1, Q^0 = 1, and 1 itself, in Montgomery form
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(lc.lv0, h.v0.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(lc.lv1, h.x0.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(lc.lqk, h.x0.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(lc.lone, h.x0.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
+        }
         if (ce == cudaSuccess) ce = cudaMemcpyAsync((void *)j.npl, h.npl.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
         if (ce == cudaSuccess) ce = cudaMemcpyAsync((void *)j.nl, h.nl.data(), H * 4, cudaMemcpyHostToDevice, e->stream);
         if (ce == cudaSuccess)
@@ -642,6 +975,8 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     }
     cudaError_t ce = cudaSuccess;
     if (!rc) ce = cudaMemcpyAsync(b->d_jobs, b->jobs.data(), n * sizeof(JobDev), cudaMemcpyHostToDevice, e->stream);
+    if (!rc && ce == cudaSuccess && mode == 2)
+        ce = cudaMemcpyAsync(b->d_lucas, b->lucas.data(), n * sizeof(LucasDev), cudaMemcpyHostToDevice, e->stream);
     if (!rc && ce != cudaSuccess) rc = pfb::cuda_fail(ce, "job upload", __FILE__, __LINE__);
     if (!rc && b->n_ok) {
         prep_kernel<<<n, THREADS, smem_bytes(b->maxlog), e->stream>>>(b->d_jobs, nullptr, e->tw);
@@ -706,8 +1041,8 @@ int batch_results(pfb_mr_batch *b, int8_t *verdict, uint16_t *residue, int resid
     int rc = PFB_OK;
     for (int i = 0; i < b->n; i++) {
         const JobDev &j = b->jobs[i];
-        if (!b->hp[i].ok) {
-            if (verdict) verdict[i] = -1;
+        if (!b->hp[i].ok || b->hp[i].decided >= 0) {
+            if (verdict) verdict[i] = (int8_t)(b->hp[i].ok ? b->hp[i].decided : -1);
             if (residue) memset(residue + (size_t)i * residue_stride, 0, sizeof(uint16_t) * residue_stride);
             continue;
         }
@@ -716,8 +1051,8 @@ int batch_results(pfb_mr_batch *b, int8_t *verdict, uint16_t *residue, int resid
             rc = PFB_E_STATE;
             continue;
         }
-        if (verdict) verdict[i] = (int8_t)(b->mode == 1 ? j.verdict : 0);
-        if (residue) {
+        if (verdict) verdict[i] = (int8_t)(b->mode >= 1 ? j.verdict : 0);
+        if (residue && b->mode != 2) {
             const size_t H = b->hp[i].x0.size();
             r22.resize(H);
             PFB_CUDA(cudaMemcpy(r22.data(), j.res, H * 4, cudaMemcpyDeviceToHost));
@@ -758,6 +1093,14 @@ int run_jobs(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int m
 extern "C" int pfb_mr_test(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base, int8_t *verdict,
                            uint16_t *residue, int residue_stride) {
     return run_jobs(e, nums, n, base, 1, nullptr, verdict, residue, residue_stride);
+}
+
+extern "C" int pfb_mr_lucas(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, int8_t *verdict) {
+    if (!verdict) {
+        pfb::set_error("pfb_mr_lucas: verdict is required");
+        return PFB_E_ARG;
+    }
+    return run_jobs(e, nums, n, 2u, 2, nullptr, verdict, nullptr, 0);
 }
 
 extern "C" int pfb_mr_powm(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, uint32_t base,

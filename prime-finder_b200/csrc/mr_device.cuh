@@ -423,12 +423,12 @@ __device__ __forceinline__ unsigned long long crt(uint32_t r1, uint32_t r2, int 
 
 // Pointwise Montgomery product of a transform in shared memory with a stored
 // spectrum in global memory (16-byte loads, 4 consecutive points per thread).
-template <int PR>
+template <int PR, bool CG = false>
 __device__ __forceinline__ void pointwise1(uint32_t *A, const uint32_t *__restrict__ C, int n, const CrtConsts &cc) {
     constexpr uint32_t p = PR ? P2 : P1;
     const uint4 *C4 = reinterpret_cast<const uint4 *>(C);
     for (int i4 = threadIdx.x; i4 < (n >> 2); i4 += blockDim.x) {
-        const uint4 c = __ldg(C4 + i4);
+        const uint4 c = CG ? __ldcg(C4 + i4) : __ldg(C4 + i4);
         const int i = 4 * i4;
         A[pad(i)] = mont(A[pad(i)], c.x, p, cc.pinv[PR]);
         A[pad(i + 1)] = mont(A[pad(i + 1)], c.y, p, cc.pinv[PR]);
@@ -438,12 +438,15 @@ __device__ __forceinline__ void pointwise1(uint32_t *A, const uint32_t *__restri
     __syncthreads();
 }
 
+// CG: the operand was written earlier in the same launch (L2-coherent loads).
+template <bool CG = false>
 __device__ __forceinline__ void pointwise2(uint32_t *A0, uint32_t *A1, const uint32_t *__restrict__ C0,
                                            const uint32_t *__restrict__ C1, int n, const CrtConsts &cc) {
     const uint4 *C04 = reinterpret_cast<const uint4 *>(C0);
     const uint4 *C14 = reinterpret_cast<const uint4 *>(C1);
     for (int i4 = threadIdx.x; i4 < (n >> 2); i4 += blockDim.x) {
-        const uint4 c = __ldg(C04 + i4), d = __ldg(C14 + i4);
+        const uint4 c = CG ? __ldcg(C04 + i4) : __ldg(C04 + i4);
+        const uint4 d = CG ? __ldcg(C14 + i4) : __ldg(C14 + i4);
         const int i = 4 * i4;
         A0[pad(i)] = mont(A0[pad(i)], c.x, P1, cc.pinv[0]);
         A0[pad(i + 1)] = mont(A0[pad(i + 1)], c.y, P1, cc.pinv[0]);
@@ -470,17 +473,22 @@ struct Smem {
 };
 
 // One Montgomery step on X (H limbs): X <- REDC(X^2) * a   (square = true)
+//                                   or X <- REDC(X * Y) * a  (gy = spectrum of Y)
 //                                   or X <- REDC(X)           (square = false).
-// On entry X < 4N (or < R for square = false); on exit X < 2N * a.
+// gy holds NTT_L(Y) of both primes ([2][L], reduced), written earlier in the
+// same launch.  On entry X, Y < B N with R > B^2 N (B = 4 for the strong
+// test's squarings), or X < R for a plain REDC; on exit X < 2N * a.
+// MUL = false compiles the squaring / REDC forms only (gy ignored).
+template <bool MUL = false>
 __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                          const CrtConsts &cc) {
+                          const CrtConsts &cc, const uint32_t *gy = nullptr) {
     const int logl = cd.logl, L = 1 << logl, H = L >> 1;
     uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
     CarrySmem &cs = *sm.cs;
     const int tid = threadIdx.x, T = blockDim.x;
     unsigned long long cS = 0;  // carry of T_lo + T_hi
 
-    if (square) {
+    if (square || (MUL && gy)) {
         for (int i = tid; i < L; i += T) {
             const uint32_t v = i < H ? X[pad(i)] : 0u;
             A0[pad(i)] = v;
@@ -488,15 +496,19 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
         }
         __syncthreads();
         dif(A0, A1, logl, tw);
-        for (int i = tid; i < L; i += T) {
-            const int q = pad(i);
-            const uint32_t u = A0[q], v = A1[q];
-            A0[q] = mont(u, u, P1, cc.pinv[0]);
-            A1[q] = mont(v, v, P2, cc.pinv[1]);
+        if (MUL && gy) {
+            pointwise2<true>(A0, A1, gy, gy + L, L, cc);
+        } else {
+            for (int i = tid; i < L; i += T) {
+                const int q = pad(i);
+                const uint32_t u = A0[q], v = A1[q];
+                A0[q] = mont(u, u, P1, cc.pinv[0]);
+                A1[q] = mont(v, v, P2, cc.pinv[1]);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         dit(A0, A1, logl, tw);
-        // T = x^2 as L limbs, in place over A0
+        // T = x^2 (or x y) as L limbs, in place over A0
         carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
         // S1 = T_lo + T_hi  -> X, carry cS
         cS = carry_pass<true>(H, 0ull,
@@ -550,8 +562,9 @@ __device__ __forceinline__ uint32_t ldg_spill(const uint32_t *p) { return __ldcg
 // mont_step for transforms too long for both primes to sit in shared memory
 // (L = 2^15): the p1 spectrum makes a round trip through global memory (L2).
 // Same arithmetic and result as mont_step; sm.A1 is unused.
+template <bool MUL = false>
 __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                              const CrtConsts &cc, const Spill &sp) {
+                              const CrtConsts &cc, const Spill &sp, const uint32_t *gy = nullptr) {
     const int logl = cd.logl, L = 1 << logl, H = L >> 1;
     uint32_t *A = sm.A0, *X = sm.X;
     CarrySmem &cs = *sm.cs;
@@ -565,23 +578,31 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
         for (int i = tid; i < n; i += T) sp.s[i] = A[pad(i)];
         __syncthreads();
     };
-    if (square) {
+    if (square || (MUL && gy)) {
         load_x(X, false);
         dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
-        for (int i = tid; i < L; i += T) {
-            const uint32_t u = A[pad(i)];
-            A[pad(i)] = mont(u, u, P1, cc.pinv[0]);
+        if (MUL && gy) {
+            pointwise1<0, true>(A, gy, L, cc);
+        } else {
+            for (int i = tid; i < L; i += T) {
+                const uint32_t u = A[pad(i)];
+                A[pad(i)] = mont(u, u, P1, cc.pinv[0]);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         dit1<0>(A, logl, tw.wi[0], tw.wish[0]);
         spill(L);
         load_x(X, false);
         dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
-        for (int i = tid; i < L; i += T) {
-            const uint32_t u = A[pad(i)];
-            A[pad(i)] = mont(u, u, P2, cc.pinv[1]);
+        if (MUL && gy) {
+            pointwise1<1, true>(A, gy + L, L, cc);
+        } else {
+            for (int i = tid; i < L; i += T) {
+                const uint32_t u = A[pad(i)];
+                A[pad(i)] = mont(u, u, P2, cc.pinv[1]);
+            }
+            __syncthreads();
         }
-        __syncthreads();
         dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
         carry_pass<true>(L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
         cS = carry_pass<true>(H, 0ull,

@@ -10,7 +10,9 @@
 #include <vector>
 
 #include "batch_mod_ctx.cuh"
+#include "common.cuh"
 #include "bigint_host.h"
+#include "phase2_host.h"
 #include "miller_rabin.h"
 #include "miller_rabin_runner.cuh"
 #include "pfb_mr.h"
@@ -76,63 +78,30 @@ namespace {
 std::mutex g_mu;
 std::vector<pfb_mr_t *> g_eng;
 
-int ndig(int x) { return x < 10 ? 1 : x < 100 ? 2 : x < 1000 ? 3 : 4; }
-int revd(int x, int l) {
-    int r = 0;
-    for (int i = 0; i < l; i++) {
-        r = r * 10 + x % 10;
-        x /= 10;
-    }
-    return r;
-}
-
-// 10^a - m1*10^e1 - m2*10^e2 - 1 (miller_rabin.c:56-99); empty on bad input.
-pfb::big::Words build(long long a, long long e1, int m1, long long e2, int m2) {
-    using namespace pfb::big;
-    if (a < 1 || e1 < 0 || e2 < 0 || m1 < 0 || m2 < 0) return Words();
-    Words n = pow10((uint64_t)a);
-    const Words t1 = mul_small(pow10((uint64_t)e1), (uint64_t)m1);
-    const Words t2 = mul_small(pow10((uint64_t)e2), (uint64_t)m2);
-    Words one(1, 1);
-    Words s = t1;
-    {  // s = t1 + t2 + 1
-        Words r(std::max(t1.size(), t2.size()) + 1, 0);
-        unsigned __int128 carry = 1;
-        for (size_t i = 0; i < r.size(); i++) {
-            carry += (unsigned __int128)(i < t1.size() ? t1[i] : 0) + (i < t2.size() ? t2[i] : 0);
-            r[i] = (uint64_t)carry;
-            carry >>= 64;
-        }
-        trim(r);
-        s = r;
-    }
-    if (cmp(n, s) <= 0) return Words();
-    return sub(n, s);
-}
-
-// Strong probable-prime rounds to 2, 3, 5, 7, 11 (bases that are multiples of
-// a tiny N are skipped); even N and N < 2 are answered directly.
-int prp(pfb_mr_t *e, const pfb::big::Words &N) {
-    const size_t bits = pfb::big::bit_length(N);
-    if (bits <= 1) return 0;                      // 0 or 1
-    if (!(N[0] & 1ull)) return bits == 2 ? 1 : 0;  // 2 is prime, other even N are not
-    std::vector<uint16_t> l16((bits + 15) / 16);
-    pfb::big::to_u16(N, l16.data(), l16.size());
-    const pfb_mr_number_t num{l16.data(), (int)l16.size()};
-    for (uint32_t base : {2u, 3u, 5u, 7u, 11u}) {
-        if (bits <= 4 && base % N[0] == 0) continue;
-        int8_t v = -1;
-        if (pfb_mr_test(e, &num, 1, base, &v, nullptr, 0) != PFB_OK) return -1;
-        if (v != 1) return v < 0 ? -1 : 0;
-    }
-    return 1;
-}
-
 double secs(std::chrono::steady_clock::time_point a, std::chrono::steady_clock::time_point b) {
     return std::chrono::duration<double>(b - a).count();
 }
 
 }  // namespace
+
+extern "C" int pfb_mr_bpsw(pfb_mr_t *e, const pfb_mr_number_t *nums, int n, int8_t *verdict) {
+    if (!e || !nums || n <= 0 || !verdict) {
+        pfb::set_error("pfb_mr_bpsw: bad argument");
+        return PFB_E_ARG;
+    }
+    std::vector<pfb::big::Words> w(n);
+    for (int i = 0; i < n; i++) {
+        if (!nums[i].limbs || nums[i].n_limbs <= 0) {
+            pfb::set_error("pfb_mr_bpsw: number %d has no limbs", i);
+            return PFB_E_ARG;
+        }
+        w[i] = pfb::big::from_u16(nums[i].limbs, (size_t)nums[i].n_limbs);
+    }
+    const std::vector<int> v = pfb::phase2::prp_batch(e, w);
+    if (v.empty()) return PFB_E_CUDA;
+    for (int i = 0; i < n; i++) verdict[i] = (int8_t)v[i];
+    return PFB_OK;
+}
 
 extern "C" int miller_rabin_test(long long a, long long b, long long c, int k, int j, mr_timing_t *timing) {
     if (timing) *timing = mr_timing_t{0.0, 0.0, 0.0, 0.0};
@@ -148,21 +117,22 @@ extern "C" int miller_rabin_test(long long a, long long b, long long c, int k, i
     }
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
-    const pfb::big::Words N = build(a, b, k, c, j);
+    const pfb::big::Words N = pfb::phase2::build_n(a, b, c, k, j);
     const auto t1 = clk::now();
     if (N.empty()) return -1;
-    const int rN = prp(e, N);
+    const std::vector<int> vN = pfb::phase2::prp_batch(e, {N});
+    const int rN = vN.empty() ? -1 : vN[0];
     const auto t2 = clk::now();
     if (timing) {
         timing->build_n = secs(t0, t1);
         timing->mr_n = secs(t1, t2);
     }
     if (rN <= 0) return rN;
-    const int lk = ndig(k), lj = ndig(j);
-    const pfb::big::Words R = build(a, a - b - lk, revd(k, lk), a - c - lj, revd(j, lj));
+    const pfb::big::Words R = pfb::phase2::build_rev(a, b, c, k, j);
     const auto t3 = clk::now();
     if (R.empty()) return -1;
-    const int rR = prp(e, R);
+    const std::vector<int> vR = pfb::phase2::prp_batch(e, {R});
+    const int rR = vR.empty() ? -1 : vR[0];
     const auto t4 = clk::now();
     if (timing) {
         timing->build_revn = secs(t2, t3);

@@ -248,6 +248,9 @@ def _mr_lib():
         L.pfb_mr_powm.argtypes = [vp, C.POINTER(_Number), C.c_int, C.c_uint32,
                                   C.POINTER(_Number), C.POINTER(C.c_uint16), C.c_int]
         L.pfb_mr_powm.restype = C.c_int
+        for fn in (L.pfb_mr_lucas, L.pfb_mr_bpsw):
+            fn.argtypes = [vp, C.POINTER(_Number), C.c_int, C.POINTER(C.c_int8)]
+            fn.restype = C.c_int
         L.pfb_mr_test_cost.argtypes = [C.POINTER(C.c_uint16), C.c_int]
         L.pfb_mr_test_cost.restype = C.c_longlong
         L._mr_ready = True
@@ -290,6 +293,22 @@ class MillerRabin:
         if residues:
             out = [limbs16_to_int(res[i * stride:(i + 1) * stride]) for i in range(n)]
         return ver.tolist(), out
+
+    def _verdicts(self, fn, name, numbers):
+        st, keep = _numbers(numbers)
+        ver = np.zeros(len(keep), dtype=np.int8)
+        _check(fn(self._h, st, len(keep), ver.ctypes.data_as(C.POINTER(C.c_int8))), name)
+        return ver.tolist()
+
+    def lucas(self, numbers):
+        """Strong Lucas test (Selfridge's parameters) per number (pfb_mr_lucas):
+        1 strong Lucas probable prime, 0 composite, -1 invalid."""
+        return self._verdicts(_mr_lib().pfb_mr_lucas, "pfb_mr_lucas", numbers)
+
+    def bpsw(self, numbers):
+        """Baillie-PSW per number (pfb_mr_bpsw): 1 probable prime, 0 composite,
+        -1 too long."""
+        return self._verdicts(_mr_lib().pfb_mr_bpsw, "pfb_mr_bpsw", numbers)
 
     def powm(self, numbers, exps, base: int = 2):
         st, keep = _numbers(numbers)
@@ -502,3 +521,69 @@ class MRServer:
 
 def batch_steps_done(batch: "MRBatch") -> int:
     return int(_server_lib().pfb_mr_batch_steps_done(batch._h))
+
+
+# ---------------------------------------------------------------- pipeline ---
+
+class Phase2Record(C.Structure):
+    """pfb_phase2_record_t"""
+    _fields_ = [("a", C.c_longlong), ("b", C.c_longlong), ("c", C.c_longlong), ("k", C.c_int),
+                ("j", C.c_int), ("result", C.c_int)]
+
+
+class PipelineConfig(C.Structure):
+    """pfb_pipeline_config_t"""
+    _fields_ = [("K", C.c_int), ("triples_per_sieve", C.c_int), ("max_resident", C.c_int),
+                ("hbm_budget_bytes", C.c_size_t), ("prep_threads", C.c_int), ("window", C.c_int)]
+
+
+class PipelineStats(C.Structure):
+    """pfb_pipeline_stats_t"""
+    _fields_ = [("triples", C.c_longlong), ("survivors", C.c_longlong), ("n_prp", C.c_longlong),
+                ("rev_tested", C.c_longlong), ("both_prp", C.c_longlong), ("invalid", C.c_longlong),
+                ("sieve_s", C.c_double), ("phase2_s", C.c_double), ("total_s", C.c_double)]
+
+
+def _pipeline_lib():
+    L = _mr_lib()
+    if not hasattr(L, "_pipeline_ready"):
+        L.pfb_pipeline_run.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_longlong), C.c_int,
+                                       C.POINTER(PipelineConfig), C.POINTER(C.c_uint8),
+                                       C.POINTER(Phase2Record), C.c_longlong, C.POINTER(C.c_longlong),
+                                       C.POINTER(PipelineStats)]
+        L.pfb_pipeline_run.restype = C.c_int
+        L.pfb_mr_device.argtypes = [C.c_void_p]
+        L.pfb_mr_device.restype = C.c_int
+        L._pipeline_ready = True
+    return L
+
+
+def pipeline_run(sieve: "Sieve", engine: "MillerRabin", abc, K: int, pre_mask: Optional[np.ndarray] = None,
+                 cap: Optional[int] = None, triples_per_sieve: int = 0, max_resident: int = 0,
+                 hbm_budget_bytes: int = 0, prep_threads: int = 0, window: int = 0):
+    """Sieve the triples on the K x K grid and decide every survivor
+    (pfb_pipeline_run).  Returns ([(a, b, c, k, j, result), ...], stats)
+    with miller_rabin_test result codes, triple order, k-major."""
+    L = _pipeline_lib()
+    flat, pabc, n = _abc_array(abc)
+    cfg = PipelineConfig(K, triples_per_sieve, max_resident, hbm_budget_bytes, prep_threads, window)
+    pm = None
+    if pre_mask is not None:
+        pre_mask = np.ascontiguousarray(pre_mask, dtype=np.uint8)
+        if pre_mask.size < mask_bytes(K) * n:
+            raise ValueError("pre_mask holds fewer than n_abc mask blocks")
+        pm = pre_mask.ctypes.data_as(C.POINTER(C.c_uint8))
+    st = PipelineStats()
+    n_out = C.c_longlong(0)
+    if cap is None:
+        # count first: a zero-capacity call sieves and reports the survivors
+        rc = L.pfb_pipeline_run(sieve._h, engine._h, pabc, n, C.byref(cfg), pm, None, 0, C.byref(n_out),
+                                C.byref(st))
+        if rc not in (PFB_OK, -4):
+            raise PfbError(rc, "pfb_pipeline_run")
+        cap = n_out.value
+    out = (Phase2Record * max(1, cap))()
+    _check(L.pfb_pipeline_run(sieve._h, engine._h, pabc, n, C.byref(cfg), pm, out, cap, C.byref(n_out),
+                              C.byref(st)), "pfb_pipeline_run")
+    recs = [(r.a, r.b, r.c, r.k, r.j, r.result) for r in out[:n_out.value]]
+    return recs, {f: getattr(st, f) for f, _ in PipelineStats._fields_}
