@@ -299,6 +299,9 @@ def main():
             stream.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
     sieve_pairs_s = ntr * K * K * len(times) / max_over_ranks(sum(times)) * world
+    # compulsory HBM bytes of one triple: the prime list read once, the mask written once
+    sieve_bytes = 4 * len(primes) + pfb200.mask_bytes(K)
+    sieve_gbs = sieve_bytes * ntr * len(times) / max_over_ranks(sum(times)) / 1e9
     t = pfb200.GpuTiming()
     pfb200.trial_div_gpu(primes, *abc1, None, t)
     t0 = time.perf_counter()
@@ -311,10 +314,17 @@ def main():
     cands = [pfb200.build_candidate(*abc1, k, j, rev) for (k, j) in pairs for rev in (False, True)]
     sq_per_test = statistics.mean([(N - 1).bit_length() for N in cands])  # bits(d) + 1 check, s = 1
     eng = pfb200.MillerRabin(dev)
+    # per-length tuning of the persistent kernel (quantum, steps per launch)
+    tune = eng.autotune(14, 15)
+    autotune = {"chosen": {str(k): {"quantum": v[0], "chunk": v[1]} for k, v in tune["chosen"].items()},
+                "tried": [[r["logl"], r["quantum"], r["chunk"], round(r["squarings_per_s_1"]),
+                           round(r["squarings_per_s_2"])] for r in tune["tried"]],
+                "columns": "logl, quantum, chunk, squarings/s at 1 and at 2 candidates per SM"}
     batch = pfb200.MRBatch(eng, cands, 2)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     chunk = args.chunk
-    launches_per_step = (chunk + 2047) // 2048
+    tuned_chunk = eng.tuning(14)[1]
+    launches_per_step = (chunk + tuned_chunk - 1) // tuned_chunk
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             batch.advance(chunk, stream.cuda_stream)
@@ -486,7 +496,10 @@ def main():
         "plain": {"value": plain_tests_s, "unit": "tests/s", "form": "one candidate per call"},
         "served_over_plain": tests_s / world / plain_tests_s,
         "uneven": uneven,
+        "autotune": autotune,
         "sieve": {"value": sieve_pairs_s, "unit": "pairs/s", "K": K, "triples_per_step": ntr,
+                  "ms_per_triple": 1e3 / (sieve_pairs_s / world / (K * K)),
+                  "hbm_compulsory_gbs": sieve_gbs, "hbm_compulsory_bytes_per_triple": sieve_bytes,
                   "dropin_100x100_s": dropin_s, "dropin_timing": {"upload": t.upload, "kernel": t.kernel,
                                                                   "download": t.download}},
         "roofline": roofline,

@@ -165,6 +165,28 @@ long long pfb_mr_test_cost(const uint16_t *limbs, int n_limbs);
  * kernel.  No counterpart in the reference (a measurement utility). */
 int pfb_measure_int32_peak(int device, double *mul_lo_per_s, double *mul_hi_per_s);
 
+/*
+ * Autotuner of the persistent squaring kernel, per transform-length bucket
+ * (log2 L from logl_lo to logl_hi, within 8..15; a 50 000-digit modulus is
+ * 14, 100 000 digits 15).  For each bucket it times 2048 squarings of
+ * synthetic moduli of the bucket's largest size, in batches of one and of two
+ * candidates per SM, for every pair (quantum: steps of one candidate per
+ * scheduling quantum, 32 to 256; chunk: steps per launch, 1024 or 2048), and
+ * keeps in the engine, for every later batch of that bucket, the pair with
+ * the best sum over the two shapes of its rate relative to the shape's best.
+ * results (optional, cap rows) receives one row per pair; *n_results the rows
+ * written.  The defaults before tuning are quantum 64, chunk 2048.
+ */
+typedef struct {
+    int logl, quantum, chunk;
+    double squarings_per_s_1;   /* whole device, one candidate per SM  */
+    double squarings_per_s_2;   /* whole device, two candidates per SM */
+} pfb_mr_tune_t;
+int pfb_mr_autotune(pfb_mr_t *e, int logl_lo, int logl_hi, pfb_mr_tune_t *results, int cap,
+                    int *n_results);
+/* The (quantum, chunk) pair the engine uses for transform length 2^logl. */
+int pfb_mr_get_tuning(pfb_mr_t *e, int logl, int *quantum, int *chunk);
+
 #ifdef __cplusplus
 }
 #endif

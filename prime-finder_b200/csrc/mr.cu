@@ -645,6 +645,10 @@ struct pfb_mr {
     uint32_t *d_tw = nullptr;
     uint32_t *d_wide = nullptr;
     Twiddles tw{};
+    // persistent-kernel parameters per transform length (pfb_mr_autotune):
+    // steps of one candidate per quantum, steps per launch
+    int quantum[LOG_LMAX + 1];
+    int chunk[LOG_LMAX + 1];
 };
 
 static int build_tables(pfb_mr *e) {
@@ -744,6 +748,10 @@ extern "C" int pfb_mr_create(pfb_mr_t **out, int device) {
     *out = nullptr;
     pfb_mr *e = new pfb_mr();
     e->device = device;
+    for (int lg = 0; lg <= LOG_LMAX; lg++) {
+        e->quantum[lg] = 64;
+        e->chunk[lg] = 2048;
+    }
     int rc = PFB_OK;
     cudaError_t ce = cudaSetDevice(device);
     if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "cudaSetDevice", __FILE__, __LINE__);
@@ -865,9 +873,64 @@ struct pfb_mr_batch {
     std::vector<HostPrep> hp;
     std::vector<JobDev> jobs;
     std::vector<LucasDev> lucas;
+    struct Graph {
+        long long chunk;
+        int quantum;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;  // one launch of the persistent kernel per (chunk, quantum)
 };
 
 namespace {
+
+void batch_free(pfb_mr_batch *b) {
+    for (auto &g : b->graphs) cudaGraphExecDestroy(g.exec);
+    cudaFree(b->d_arena);
+    delete b;
+}
+
+// One step chunk of a batch -- the quanta counter reset and the persistent
+// kernel -- as a CUDA graph, built on first use per (chunk, quantum) and
+// replayed by every later advance of the batch.
+int chunk_graph(pfb_mr_batch *b, long long chunk, int quantum, cudaGraphExec_t *out) {
+    for (const auto &g : b->graphs)
+        if (g.chunk == chunk && g.quantum == quantum) {
+            *out = g.exec;
+            return PFB_OK;
+        }
+    JobDev *jobs = b->d_jobs;
+    int n = b->n, q = quantum;
+    int *locks = b->d_locks;
+    unsigned int *counter = b->d_counter;
+    const long long qpj = (chunk + quantum - 1) / quantum;
+    unsigned int total = (unsigned int)std::min<long long>((long long)b->n * qpj, 0x7fffffffll);
+    Twiddles tw = b->e->tw;
+    void *args[] = {&jobs, &n, &locks, &counter, &total, &q, &tw};
+    cudaGraph_t graph = nullptr;
+    PFB_CUDA(cudaGraphCreate(&graph, 0));
+    cudaMemsetParams mp{};
+    mp.dst = counter;
+    mp.value = 0;
+    mp.elementSize = sizeof(unsigned int);
+    mp.width = 1;
+    mp.height = 1;
+    cudaKernelNodeParams kp{};
+    kp.func = (void *)persist_kernel;
+    kp.gridDim = dim3((unsigned)std::min(b->n, std::max(1, b->e->num_sms)));
+    kp.blockDim = dim3(THREADS);
+    kp.sharedMemBytes = (unsigned)smem_bytes(b->maxlog);
+    kp.kernelParams = args;
+    cudaGraphNode_t n_mem = nullptr, n_ker = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaError_t ce = cudaGraphAddMemsetNode(&n_mem, graph, nullptr, 0, &mp);
+    if (ce == cudaSuccess) ce = cudaGraphAddKernelNode(&n_ker, graph, &n_mem, 1, &kp);
+    if (ce == cudaSuccess) ce = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ce != cudaSuccess) return pfb::cuda_fail(ce, "chunk graph", __FILE__, __LINE__);
+    b->graphs.push_back(pfb_mr_batch::Graph{chunk, quantum, exec});
+    *out = exec;
+    return PFB_OK;
+}
 
 int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int mode,
                 const pfb_mr_number_t *exps, pfb_mr_batch **out) {
@@ -911,8 +974,7 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
     }
     uint32_t *d_words = (uint32_t *)(b->d_arena + job_bytes + lock_bytes + lucas_bytes);
     if (cudaMemsetAsync(b->d_locks, 0, lock_bytes, e->stream) != cudaSuccess) {
-        cudaFree(b->d_arena);
-        delete b;
+        batch_free(b);
         return pfb::cuda_fail(cudaGetLastError(), "lock reset", __FILE__, __LINE__);
     }
     b->jobs.assign(n, JobDev{});
@@ -989,8 +1051,7 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
         if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "batch sync", __FILE__, __LINE__);
     }
     if (rc) {
-        cudaFree(b->d_arena);
-        delete b;
+        batch_free(b);
         return rc;
     }
     *out = b;
@@ -1001,17 +1062,15 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
 // persistent kernel, each handing out n * ceil(chunk / quantum) quanta.
 int batch_advance(pfb_mr_batch *b, long long steps, cudaStream_t st) {
     if (!b->n_ok || steps <= 0) return PFB_OK;
-    const size_t sm = smem_bytes(b->maxlog);
-    const int grid = std::min(b->n, std::max(1, b->e->num_sms));
+    const long long cmax = b->e->chunk[b->maxlog];
+    const int q0 = b->e->quantum[b->maxlog];
     while (steps > 0) {
-        const long long chunk = std::min<long long>(steps, 2048);
-        const int quantum = (int)std::min<long long>(chunk, 64);
-        const long long qpj = (chunk + quantum - 1) / quantum;
-        const unsigned int total = (unsigned int)std::min<long long>((long long)b->n * qpj, 0x7fffffffll);
-        PFB_CUDA(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned int), st));
-        persist_kernel<<<grid, THREADS, sm, st>>>(b->d_jobs, b->n, b->d_locks, b->d_counter, total, quantum,
-                                                  b->e->tw);
-        PFB_CUDA(cudaGetLastError());
+        const long long chunk = std::min<long long>(steps, cmax);
+        const int quantum = (int)std::min<long long>(chunk, q0);
+        cudaGraphExec_t g = nullptr;
+        const int rc = chunk_graph(b, chunk, quantum, &g);
+        if (rc) return rc;
+        PFB_CUDA(cudaGraphLaunch(g, st));
         steps -= chunk;
         b->steps_done += chunk;
     }
@@ -1083,8 +1142,7 @@ int run_jobs(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int m
     }
     if (!rc) rc = batch_results(b, verdict, residue, residue_stride);
     cudaStreamSynchronize(e->stream);
-    cudaFree(b->d_arena);
-    delete b;
+    batch_free(b);
     return rc;
 }
 
@@ -1166,8 +1224,107 @@ extern "C" void pfb_mr_batch_destroy(pfb_mr_batch_t *b) {
     if (!b) return;
     cudaSetDevice(b->e->device);
     cudaDeviceSynchronize();
-    cudaFree(b->d_arena);
-    delete b;
+    batch_free(b);
+}
+
+extern "C" int pfb_mr_autotune(pfb_mr_t *e, int logl_lo, int logl_hi, pfb_mr_tune_t *results, int cap,
+                               int *n_results) {
+    if (!e || logl_lo < LOG_LMIN || logl_hi > LOG_LSEQ || logl_lo > logl_hi || (cap > 0 && !results)) {
+        pfb::set_error("pfb_mr_autotune: bad argument (transform lengths 2^%d .. 2^%d)", LOG_LMIN, LOG_LSEQ);
+        return PFB_E_ARG;
+    }
+    if (n_results) *n_results = 0;
+    PFB_CUDA(cudaSetDevice(e->device));
+    static const int kQuanta[] = {32, 64, 128, 256};
+    static const int kChunks[] = {1024, 2048};
+    constexpr int NQ = 4, NC = 2, NP = NQ * NC;
+    const long long kSteps = 2048;  // timed steps per tried pair and batch shape
+    const int sms = std::max(1, e->num_sms);
+    int rows = 0;
+    uint64_t x = 0x9E3779B97F4A7C15ull;  // xorshift64: synthetic moduli
+    cudaEvent_t ev[2];
+    PFB_CUDA(cudaEventCreate(&ev[0]));
+    PFB_CUDA(cudaEventCreate(&ev[1]));
+    int rc = PFB_OK;
+    for (int lg = logl_lo; lg <= logl_hi && !rc; lg++) {
+        // the longest base-2 modulus of this length: R = 2^(22 L/2) >= 2^(bits + 6)
+        const size_t bits = std::min<size_t>((size_t)LIMB_BITS * ((size_t)1 << (lg - 1)) - 8, PFB_MR_MAX_BITS);
+        const int n16 = (int)((bits + 15) / 16);
+        const int q_old = e->quantum[lg], c_old = e->chunk[lg];
+        double rate[2][NP] = {};
+        // two batch shapes: one and two candidates per SM (the tail of a launch
+        // weighs more with one)
+        for (int shape = 0; shape < 2 && !rc; shape++) {
+            const int n = (shape + 1) * sms;
+            std::vector<uint16_t> limbs((size_t)n * n16);
+            std::vector<pfb_mr_number_t> nums(n);
+            for (int i = 0; i < n; i++) {
+                uint16_t *l = limbs.data() + (size_t)i * n16;
+                for (int w = 0; w < n16; w++) {
+                    x ^= x << 13;
+                    x ^= x >> 7;
+                    x ^= x << 17;
+                    l[w] = (uint16_t)x;
+                }
+                const int top = (int)((bits - 1) % 16);
+                l[n16 - 1] = (uint16_t)((l[n16 - 1] & ((1u << top) - 1u)) | (1u << top));
+                l[0] |= 1u;
+                nums[i] = pfb_mr_number_t{l, n16};
+            }
+            pfb_mr_batch *b = nullptr;
+            rc = batch_build(e, nums.data(), n, 2u, 1, nullptr, &b);
+            if (rc) break;
+            rc = batch_advance(b, 64, e->stream);  // warm-up
+            for (int k = 0; k < NP && !rc; k++) {
+                e->quantum[lg] = kQuanta[k / NC];
+                e->chunk[lg] = kChunks[k % NC];
+                long long before = 0, after = 0;
+                rc = batch_pending(b, nullptr, &before);
+                if (!rc && cudaEventRecord(ev[0], e->stream) != cudaSuccess) rc = PFB_E_CUDA;
+                if (!rc) rc = batch_advance(b, kSteps, e->stream);
+                if (!rc && cudaEventRecord(ev[1], e->stream) != cudaSuccess) rc = PFB_E_CUDA;
+                if (!rc) rc = batch_pending(b, nullptr, &after);
+                float ms = 0.f;
+                if (!rc && cudaEventElapsedTime(&ms, ev[0], ev[1]) != cudaSuccess) rc = PFB_E_CUDA;
+                if (!rc) rate[shape][k] = ms > 0.f ? (double)(after - before) / (1e-3 * (double)ms) : 0.0;
+            }
+            batch_free(b);
+        }
+        e->quantum[lg] = q_old;
+        e->chunk[lg] = c_old;
+        if (rc) break;
+        // score: the sum over shapes of the rate relative to the shape's best
+        double best_rate[2] = {0.0, 0.0}, best = -1.0;
+        for (int shape = 0; shape < 2; shape++)
+            for (int k = 0; k < NP; k++) best_rate[shape] = std::max(best_rate[shape], rate[shape][k]);
+        for (int k = 0; k < NP; k++) {
+            double score = 0.0;
+            for (int shape = 0; shape < 2; shape++)
+                score += best_rate[shape] > 0.0 ? rate[shape][k] / best_rate[shape] : 0.0;
+            if (results && rows < cap)
+                results[rows] = pfb_mr_tune_t{lg, kQuanta[k / NC], kChunks[k % NC], rate[0][k], rate[1][k]};
+            rows++;
+            if (score > best) {
+                best = score;
+                e->quantum[lg] = kQuanta[k / NC];
+                e->chunk[lg] = kChunks[k % NC];
+            }
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    if (n_results) *n_results = std::min(rows, cap);
+    return rc;
+}
+
+extern "C" int pfb_mr_get_tuning(pfb_mr_t *e, int logl, int *quantum, int *chunk) {
+    if (!e || logl < 0 || logl > LOG_LMAX) {
+        pfb::set_error("pfb_mr_get_tuning: bad argument");
+        return PFB_E_ARG;
+    }
+    if (quantum) *quantum = e->quantum[logl];
+    if (chunk) *chunk = e->chunk[logl];
+    return PFB_OK;
 }
 
 extern "C" long long pfb_mr_test_cost(const uint16_t *limbs, int n_limbs) {

@@ -196,29 +196,61 @@ __device__ __forceinline__ void mark_global(uint32_t *mask, int K, uint32_t k, u
 // Cost: O(log p) per line plus O(1) per hit, where walking the K values of x
 // costs O(K).
 
-__device__ __forceinline__ uint32_t ceil_div64(unsigned long long n, uint32_t d) {
-    return (uint32_t)((n + d - 1ull) / d);
+// Exact quotients by d from a double estimate (rd = 1/d, one division per
+// divisor) corrected with integer arithmetic: for quotients below 2^50 the
+// estimate is within two units.
+__device__ __forceinline__ uint32_t quot32(uint32_t v, uint32_t d, double rd) {
+    uint32_t q = (uint32_t)((double)v * rd);
+    long long r = (long long)v - (long long)q * d;
+    while (r < 0) {
+        q--;
+        r += d;
+    }
+    while (r >= (long long)d) {
+        q++;
+        r -= d;
+    }
+    return q;
 }
 
+__device__ __forceinline__ unsigned long long quot64(unsigned long long n, uint32_t d, double rd) {
+    unsigned long long q = (unsigned long long)((double)n * rd);
+    long long r = (long long)(n - q * d);
+    while (r < 0) {
+        q--;
+        r += d;
+    }
+    while (r >= (long long)d) {
+        q++;
+        r -= d;
+    }
+    return q;
+}
+
+// The descent keeps, per level, the multiplier a, its reciprocal and the
+// interval start L; the level's modulus is the previous level's multiplier
+// (p at level 0).
 __device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, uint32_t Y) {
     if (c < Y) return 0u;
     uint32_t a = g, m = p, L = p - c, R = p - c + Y - 1u;
-    uint32_t sm[34], sa[34], sl[34];
+    uint32_t sa[34], sl[34];
+    double sr[34];
     int d = 0;
     uint32_t x;
     for (;;) {
-        const uint32_t k = (L - 1u) / a + 1u;  // ceil(L / a), L >= 1
+        const double rd = 1.0 / (double)a;
+        const uint32_t k = quot32(L - 1u, a, rd) + 1u;  // ceil(L / a), L >= 1
         if ((unsigned long long)a * k <= R) {
             x = k;
             break;
         }
         if (d >= 34) return 0xFFFFFFFFu;  // unreachable: the modulus halves each level
-        sm[d] = m;
         sa[d] = a;
         sl[d] = L;
+        sr[d] = rd;
         d++;
-        const uint32_t r = m % a;           // != 0: gcd(a, m) = 1 along the chain
-        uint32_t a2 = a - r, L2 = L % a, R2 = R % a;
+        const uint32_t r = m - quot32(m, a, rd) * a;  // != 0: gcd(a, m) = 1 along the chain
+        uint32_t a2 = a - r, L2 = L - quot32(L, a, rd) * a, R2 = R - quot32(R, a, rd) * a;
         const uint32_t m2 = a;
         if (a2 > (m2 >> 1)) {               // reflect: a x in [L, R] <=> (m - a) x in [m - R, m - L]
             a2 = r;
@@ -233,7 +265,8 @@ __device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, u
     }
     while (d > 0) {
         d--;
-        x = ceil_div64((unsigned long long)x * sm[d] + sl[d], sa[d]);
+        const uint32_t md = d ? sa[d - 1] : p;
+        x = (uint32_t)quot64((unsigned long long)x * md + sl[d] + sa[d] - 1u, sa[d], sr[d]);  // ceil
     }
     return x;
 }

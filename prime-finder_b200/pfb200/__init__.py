@@ -234,6 +234,12 @@ def _numbers(xs):
     return st, arrs
 
 
+class TuneRow(C.Structure):
+    """pfb_mr_tune_t"""
+    _fields_ = [("logl", C.c_int), ("quantum", C.c_int), ("chunk", C.c_int), ("squarings_per_s_1", C.c_double),
+                ("squarings_per_s_2", C.c_double)]
+
+
 def _mr_lib():
     L = lib()
     if not hasattr(L, "_mr_ready"):
@@ -251,6 +257,10 @@ def _mr_lib():
         for fn in (L.pfb_mr_lucas, L.pfb_mr_bpsw):
             fn.argtypes = [vp, C.POINTER(_Number), C.c_int, C.POINTER(C.c_int8)]
             fn.restype = C.c_int
+        L.pfb_mr_autotune.argtypes = [vp, C.c_int, C.c_int, C.POINTER(TuneRow), C.c_int, C.POINTER(C.c_int)]
+        L.pfb_mr_autotune.restype = C.c_int
+        L.pfb_mr_get_tuning.argtypes = [vp, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+        L.pfb_mr_get_tuning.restype = C.c_int
         L.pfb_mr_test_cost.argtypes = [C.POINTER(C.c_uint16), C.c_int]
         L.pfb_mr_test_cost.restype = C.c_longlong
         L._mr_ready = True
@@ -309,6 +319,23 @@ class MillerRabin:
         """Baillie-PSW per number (pfb_mr_bpsw): 1 probable prime, 0 composite,
         -1 too long."""
         return self._verdicts(_mr_lib().pfb_mr_bpsw, "pfb_mr_bpsw", numbers)
+
+    def autotune(self, logl_lo: int = 14, logl_hi: int = 15):
+        """Tune (quantum, chunk) of the persistent kernel per transform length
+        (pfb_mr_autotune).  Returns {"tried": [...], "chosen": {logl: (q, c)}}."""
+        L = _mr_lib()
+        rows = (TuneRow * 64)()
+        n = C.c_int(0)
+        _check(L.pfb_mr_autotune(self._h, logl_lo, logl_hi, rows, 64, C.byref(n)), "pfb_mr_autotune")
+        tried = [{"logl": r.logl, "quantum": r.quantum, "chunk": r.chunk,
+                  "squarings_per_s_1": r.squarings_per_s_1, "squarings_per_s_2": r.squarings_per_s_2}
+                 for r in rows[:n.value]]
+        return {"tried": tried, "chosen": {lg: self.tuning(lg) for lg in range(logl_lo, logl_hi + 1)}}
+
+    def tuning(self, logl: int):
+        q, c = C.c_int(0), C.c_int(0)
+        _check(_mr_lib().pfb_mr_get_tuning(self._h, logl, C.byref(q), C.byref(c)), "pfb_mr_get_tuning")
+        return q.value, c.value
 
     def powm(self, numbers, exps, base: int = 2):
         st, keep = _numbers(numbers)

@@ -224,3 +224,21 @@ def test_uneven_batch_subset_residues(mr):
     recs = g["records"]
     assert [(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs] == uneven_tuples(512)[:32]
     _check_records(mr, recs)
+
+
+def test_autotune_picks_a_timed_pair_and_results_hold(mr):
+    """The autotuner times every (quantum, chunk) pair of a bucket and keeps
+    the fastest; results after tuning are unchanged (the chunks replay as CUDA
+    graphs with the tuned parameters)."""
+    out = mr.autotune(12, 12)
+    rows = [r for r in out["tried"] if r["logl"] == 12]
+    assert len(rows) == 8 and all(r["squarings_per_s_1"] > 0 and r["squarings_per_s_2"] > 0 for r in rows)
+    b1 = max(r["squarings_per_s_1"] for r in rows)
+    b2 = max(r["squarings_per_s_2"] for r in rows)
+    best = max(rows, key=lambda r: r["squarings_per_s_1"] / b1 + r["squarings_per_s_2"] / b2)
+    assert out["chosen"][12] == (best["quantum"], best["chunk"])
+    rng = random.Random(41)
+    Ns = [rng.getrandbits(b) | (1 << (b - 1)) | 1 for b in (20000, 21000, 22000)]
+    ver, res = mr.test(Ns, 2)
+    for N, v, r in zip(Ns, ver, res):
+        assert r == oracle.strong_residue(N, 2)[1] and v == oracle.strong_test(N, 2)
