@@ -37,6 +37,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "prime-finder_b200"))
 sys.set_int_max_str_digits(0)
+from pfb200 import replicas  # noqa: E402
 from pfb200.workloads import serving_draw, sieve_triples, uneven_tuples, uniform_batch_pairs  # noqa: E402
 
 SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference count)
@@ -199,9 +200,7 @@ def main():
     ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
     args = ap.parse_args()
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = replicas.rank_world()
     abc1 = (50000, 30000, 100)
 
     if args.impl == "reference":
@@ -255,11 +254,7 @@ def main():
             dist.barrier()
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, dist, "cuda")
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     # primes for the sieve: generated by a plain Eratosthenes in numpy (input data)
@@ -285,7 +280,8 @@ def main():
     dmask = torch.zeros(blk * ntr, dtype=torch.uint8, device="cuda")
     sieve_launches = 0
     with torch.cuda.stream(stream):
-        triples = sieve_triples(ntr * (args.steps + args.warmup))
+        # every rank sieves its own shard of the triple enumeration (weak scaling)
+        triples = replicas.shard(sieve_triples(ntr * (args.steps + args.warmup) * world), rank, world)
         for w in range(args.warmup):
             sv.run(triples[w * ntr:(w + 1) * ntr], K, dmask, stream=stream.cuda_stream)
         stream.synchronize()
@@ -310,7 +306,7 @@ def main():
     dropin_s = (time.perf_counter() - t0) / 3
 
     # --- Miller-Rabin: resident batch ---------------------------------------
-    pairs = uniform_batch_pairs(survivors)
+    pairs = uniform_batch_pairs(survivors, seed=replicas.rank_seed(1, rank))  # each rank its own batch
     cands = [pfb200.build_candidate(*abc1, k, j, rev) for (k, j) in pairs for rev in (False, True)]
     sq_per_test = statistics.mean([(N - 1).bit_length() for N in cands])  # bits(d) + 1 check, s = 1
     eng = pfb200.MillerRabin(dev)
