@@ -171,7 +171,7 @@ int pfb_measure_int32_peak(int device, double *mul_lo_per_s, double *mul_hi_per_
  * 14, 100 000 digits 15).  For each bucket it times 2048 squarings of
  * synthetic moduli of the bucket's largest size, in batches of one and of two
  * candidates per SM, for every pair (quantum: steps of one candidate per
- * scheduling quantum, 32 to 256; chunk: steps per launch, 1024 or 2048), and
+ * scheduling quantum, 16 to 64; chunk: steps per launch, 1024 or 2048), and
  * keeps in the engine, for every later batch of that bucket, the pair with
  * the best sum over the two shapes of its rate relative to the shape's best.
  * results (optional, cap rows) receives one row per pair; *n_results the rows

@@ -1235,9 +1235,11 @@ extern "C" int pfb_mr_autotune(pfb_mr_t *e, int logl_lo, int logl_hi, pfb_mr_tun
     }
     if (n_results) *n_results = 0;
     PFB_CUDA(cudaSetDevice(e->device));
-    static const int kQuanta[] = {32, 64, 128, 256};
+    // quanta above 64 steps leave SMs idle at the end of each launch once a
+    // batch holds several candidates per SM, so the search stays below
+    static const int kQuanta[] = {16, 32, 64};
     static const int kChunks[] = {1024, 2048};
-    constexpr int NQ = 4, NC = 2, NP = NQ * NC;
+    constexpr int NQ = 3, NC = 2, NP = NQ * NC;
     const long long kSteps = 2048;  // timed steps per tried pair and batch shape
     const int sms = std::max(1, e->num_sms);
     int rows = 0;

@@ -232,7 +232,7 @@ def test_autotune_picks_a_timed_pair_and_results_hold(mr):
     graphs with the tuned parameters)."""
     out = mr.autotune(12, 12)
     rows = [r for r in out["tried"] if r["logl"] == 12]
-    assert len(rows) == 8 and all(r["squarings_per_s_1"] > 0 and r["squarings_per_s_2"] > 0 for r in rows)
+    assert len(rows) == 6 and all(r["squarings_per_s_1"] > 0 and r["squarings_per_s_2"] > 0 for r in rows)
     b1 = max(r["squarings_per_s_1"] for r in rows)
     b2 = max(r["squarings_per_s_2"] for r in rows)
     best = max(rows, key=lambda r: r["squarings_per_s_1"] / b1 + r["squarings_per_s_2"] / b2)
