@@ -117,15 +117,15 @@ __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, const in
     for (int pr = 0; pr < 2; pr++) {
         for (int i = threadIdx.x; i < L; i += blockDim.x) A[pad(i)] = i < H ? jb.npl[i] : 0u;
         __syncthreads();
-        if (pr == 0) dif1<0>(A, jb.logl, tw.w[0], tw.wsh[0]);
-        else dif1<1>(A, jb.logl, tw.w[1], tw.wsh[1]);
+        if (pr == 0) dif1<0>(A, jb.logl, tw);
+        else dif1<1>(A, jb.logl, tw);
         const uint32_t p = pr ? P2 : P1;
         for (int i = threadIdx.x; i < L; i += blockDim.x) jb.nph[pr * L + i] = red2(A[pad(i)], p);
         __syncthreads();
         for (int i = threadIdx.x; i < H; i += blockDim.x) A[pad(i)] = jb.nl[i];
         __syncthreads();
-        if (pr == 0) dif1<0>(A, jb.logl - 1, tw.w[0], tw.wsh[0]);
-        else dif1<1>(A, jb.logl - 1, tw.w[1], tw.wsh[1]);
+        if (pr == 0) dif1<0>(A, jb.logl - 1, tw);
+        else dif1<1>(A, jb.logl - 1, tw);
         for (int i = threadIdx.x; i < H; i += blockDim.x) jb.nh[pr * H + i] = red2(A[pad(i)], p);
         __syncthreads();
     }
@@ -220,8 +220,8 @@ __device__ void spectrum(const Smem &sm, int logl, const uint32_t *src, uint32_t
     for (int pr = 0; pr < 2; pr++) {
         for (int i = threadIdx.x; i < L; i += blockDim.x) A[pad(i)] = i < H ? __ldcg(src + i) : 0u;
         __syncthreads();
-        if (pr == 0) dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
-        else dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
+        if (pr == 0) dif1<0>(A, logl, tw);
+        else dif1<1>(A, logl, tw);
         const uint32_t p = pr ? P2 : P1;
         for (int i = threadIdx.x; i < L; i += blockDim.x) g[pr * L + i] = red2(A[pad(i)], p);
         __syncthreads();

@@ -113,14 +113,30 @@ __device__ __forceinline__ void load_tw(const uint32_t *__restrict__ W, const ui
     }
 }
 
-template <int PR, int RLOG>
-__device__ __forceinline__ void dif_group(uint32_t *__restrict__ A, int base, int sub, const uint32_t *tw,
-                                          const uint32_t *tws) {
+// ----- radix-2^RLOG passes --------------------------------------------------
+// Decimation in frequency forward (natural order in, bit-reversed out after
+// all passes), decimation in time inverse (bit-reversed in, natural out).
+// log2 of the length, of the first stage's half size h0 and of the thread
+// stride are template arguments, so group counts and strides are constants
+// and, for element strides that are multiples of 32, so are the padded
+// element offsets inside a group.  When every group of a thread has the same
+// j0 (all passes but the widest) its twiddles are loaded once per pass.
+
+template <int PR, int RLOG, int SUB>
+__device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, const uint32_t *tw,
+                                            const uint32_t *tws) {
     constexpr int R = 1 << RLOG;
     constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
     uint32_t v[R];
+    if constexpr (SUB % 32 == 0) {
+        constexpr int PS = SUB + SUB / 32;  // pad(base + e SUB) = pad(base) + e PS
+        const int pb = pad(base);
 #pragma unroll
-    for (int e = 0; e < R; e++) v[e] = A[pad(base + e * sub)];
+        for (int e = 0; e < R; e++) v[e] = A[pb + e * PS];
+    } else {
+#pragma unroll
+        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * SUB)];
+    }
 #pragma unroll
     for (int s = 0, t0 = 0; s < RLOG; t0 += R >> (s + 1), s++) {
         const int half = R >> (s + 1);
@@ -133,18 +149,32 @@ __device__ __forceinline__ void dif_group(uint32_t *__restrict__ A, int base, in
             v[e + half] = shoup(x - y + p2, tw[t], tws[t], p);
         }
     }
+    if constexpr (SUB % 32 == 0) {
+        constexpr int PS = SUB + SUB / 32;
+        const int pb = pad(base);
 #pragma unroll
-    for (int e = 0; e < R; e++) A[pad(base + e * sub)] = v[e];
+        for (int e = 0; e < R; e++) A[pb + e * PS] = v[e];
+    } else {
+#pragma unroll
+        for (int e = 0; e < R; e++) A[pad(base + e * SUB)] = v[e];
+    }
 }
 
-template <int PR, int RLOG>
-__device__ __forceinline__ void dit_group(uint32_t *__restrict__ A, int base, int h0, const uint32_t *tw,
-                                          const uint32_t *tws) {
+template <int PR, int RLOG, int H0>
+__device__ __forceinline__ void dit_group_t(uint32_t *__restrict__ A, int base, const uint32_t *tw,
+                                            const uint32_t *tws) {
     constexpr int R = 1 << RLOG;
     constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
     uint32_t v[R];
+    if constexpr (H0 % 32 == 0) {
+        constexpr int PS = H0 + H0 / 32;
+        const int pb = pad(base);
 #pragma unroll
-    for (int e = 0; e < R; e++) v[e] = A[pad(base + e * h0)];
+        for (int e = 0; e < R; e++) v[e] = A[pb + e * PS];
+    } else {
+#pragma unroll
+        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * H0)];
+    }
 #pragma unroll
     for (int s = 0, t0 = 0; s < RLOG; t0 += 1 << s, s++) {
         const int half = 1 << s;
@@ -158,168 +188,154 @@ __device__ __forceinline__ void dit_group(uint32_t *__restrict__ A, int base, in
             v[e + half] = red2(x - u + p2, p2);
         }
     }
+    if constexpr (H0 % 32 == 0) {
+        constexpr int PS = H0 + H0 / 32;
+        const int pb = pad(base);
 #pragma unroll
-    for (int e = 0; e < R; e++) A[pad(base + e * h0)] = v[e];
+        for (int e = 0; e < R; e++) A[pb + e * PS] = v[e];
+    } else {
+#pragma unroll
+        for (int e = 0; e < R; e++) A[pad(base + e * H0)] = v[e];
+    }
 }
 
-// Radix-2^RLOG decimation-in-frequency pass for prime PR over groups
-// g0, g0 + stride, ... (natural order in, bit-reversed out after all passes).
-// h0 = half size of the first stage.  When every group of this thread has the
-// same j0 (all passes but the widest) the twiddles are loaded once per pass.
-template <int PR, int RLOG>
-__device__ __forceinline__ void dif_pass1(uint32_t *__restrict__ A, int logn, int h0,
-                                          const uint32_t *__restrict__ W, const uint32_t *__restrict__ Wsh,
-                                          int g0, int stride) {
-    constexpr int R = 1 << RLOG;
-    const int groups = (1 << logn) >> RLOG;
-    const int sub = (2 * h0) >> RLOG;  // element stride inside a group
-    const int lh0 = 31 - __clz(h0);
+template <int PR, int RLOG, int LOGN, int LH0, int STRIDE>
+__device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint32_t *__restrict__ W,
+                                           const uint32_t *__restrict__ Wsh, int g0) {
+    constexpr int R = 1 << RLOG, H0 = 1 << LH0;
+    constexpr int GROUPS = (1 << LOGN) >> RLOG;
+    constexpr int SUB = (2 * H0) >> RLOG;
     uint32_t ta[R - 1], tsa[R - 1];
-    if (stride % sub == 0) {
-        if (RLOG == 4) load_wide<0, PR>(lh0, g0 % sub, ta, tsa);
-        else load_tw<RLOG, false>(W, Wsh, g0 % sub, sub, lh0, ta, tsa);
-        for (int gg = g0; gg < groups; gg += stride) {
-            const int block = gg / sub, j0 = gg - block * sub;
-            dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
+    if constexpr (STRIDE % SUB == 0) {  // every group of this thread has the same j0
+        if constexpr (RLOG == 4) load_wide<0, PR>(LH0, g0 % SUB, ta, tsa);
+        else load_tw<RLOG, false>(W, Wsh, g0 % SUB, SUB, LH0, ta, tsa);
+#pragma unroll 1
+        for (int gg = g0; gg < GROUPS; gg += STRIDE) {
+            const int block = gg / SUB, j0 = gg % SUB;
+            dif_group_t<PR, RLOG, SUB>(A, block * 2 * H0 + j0, ta, tsa);
         }
-        return;
-    }
-    for (int gg = g0; gg < groups; gg += stride) {
-        const int block = gg / sub, j0 = gg - block * sub;
-        if (RLOG == 4) load_wide<0, PR>(lh0, j0, ta, tsa);
-        else load_tw<RLOG, false>(W, Wsh, j0, sub, lh0, ta, tsa);
-        dif_group<PR, RLOG>(A, block * 2 * h0 + j0, sub, ta, tsa);
+    } else {
+#pragma unroll 1
+        for (int gg = g0; gg < GROUPS; gg += STRIDE) {
+            const int block = gg / SUB, j0 = gg % SUB;
+            if constexpr (RLOG == 4) load_wide<0, PR>(LH0, j0, ta, tsa);
+            else load_tw<RLOG, false>(W, Wsh, j0, SUB, LH0, ta, tsa);
+            dif_group_t<PR, RLOG, SUB>(A, block * 2 * H0 + j0, ta, tsa);
+        }
     }
 }
 
-// Radix-2^RLOG decimation-in-time pass for prime PR (bit-reversed in, natural
-// out); h0 = half size of the first (smallest) stage.
-template <int PR, int RLOG>
-__device__ __forceinline__ void dit_pass1(uint32_t *__restrict__ A, int logn, int h0,
-                                          const uint32_t *__restrict__ W, const uint32_t *__restrict__ Wsh,
-                                          int g0, int stride) {
-    constexpr int R = 1 << RLOG;
-    const int groups = (1 << logn) >> RLOG;
-    const int lh0 = 31 - __clz(h0);
+template <int PR, int RLOG, int LOGN, int LH0, int STRIDE>
+__device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint32_t *__restrict__ W,
+                                           const uint32_t *__restrict__ Wsh, int g0) {
+    constexpr int R = 1 << RLOG, H0 = 1 << LH0;
+    constexpr int GROUPS = (1 << LOGN) >> RLOG;
     uint32_t ta[R - 1], tsa[R - 1];
-    if (stride % h0 == 0) {
-        if (RLOG == 4) load_wide<1, PR>(lh0, g0 & (h0 - 1), ta, tsa);
-        else load_tw<RLOG, true>(W, Wsh, g0 & (h0 - 1), h0, lh0, ta, tsa);
-        for (int gg = g0; gg < groups; gg += stride) {
-            const int block = gg >> lh0, j0 = gg & (h0 - 1);
-            dit_group<PR, RLOG>(A, block * R * h0 + j0, h0, ta, tsa);
+    if constexpr (STRIDE % H0 == 0) {
+        if constexpr (RLOG == 4) load_wide<1, PR>(LH0, g0 & (H0 - 1), ta, tsa);
+        else load_tw<RLOG, true>(W, Wsh, g0 & (H0 - 1), H0, LH0, ta, tsa);
+#pragma unroll 1
+        for (int gg = g0; gg < GROUPS; gg += STRIDE) {
+            const int j0 = gg & (H0 - 1);
+            dit_group_t<PR, RLOG, H0>(A, (gg >> LH0) * R * H0 + j0, ta, tsa);
         }
-        return;
+    } else {
+#pragma unroll 1
+        for (int gg = g0; gg < GROUPS; gg += STRIDE) {
+            const int j0 = gg & (H0 - 1);
+            if constexpr (RLOG == 4) load_wide<1, PR>(LH0, j0, ta, tsa);
+            else load_tw<RLOG, true>(W, Wsh, j0, H0, LH0, ta, tsa);
+            dit_group_t<PR, RLOG, H0>(A, (gg >> LH0) * R * H0 + j0, ta, tsa);
+        }
     }
-    for (int gg = g0; gg < groups; gg += stride) {
-        const int j0 = gg & (h0 - 1);
-        if (RLOG == 4) load_wide<1, PR>(lh0, j0, ta, tsa);
-        else load_tw<RLOG, true>(W, Wsh, j0, h0, lh0, ta, tsa);
-        dit_group<PR, RLOG>(A, (gg >> lh0) * R * h0 + j0, h0, ta, tsa);
-    }
 }
 
-// Both primes in one pass: threads [0, T/2) work on A0 (p1), [T/2, T) on A1 (p2).
-template <int RLOG>
-__device__ __forceinline__ void dif_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
-    const int half = blockDim.x >> 1;
-    if ((int)threadIdx.x < half)
-        dif_pass1<0, RLOG>(A0, logn, h0, tw.w[0], tw.wsh[0], threadIdx.x, half);
-    else
-        dif_pass1<1, RLOG>(A1, logn, h0, tw.w[1], tw.wsh[1], threadIdx.x - half, half);
-}
-
-template <int RLOG>
-__device__ __forceinline__ void dit_pass(uint32_t *A0, uint32_t *A1, int logn, int h0, const Twiddles &tw) {
-    const int half = blockDim.x >> 1;
-    if ((int)threadIdx.x < half)
-        dit_pass1<0, RLOG>(A0, logn, h0, tw.wi[0], tw.wish[0], threadIdx.x, half);
-    else
-        dit_pass1<1, RLOG>(A1, logn, h0, tw.wi[1], tw.wish[1], threadIdx.x - half, half);
-}
-
-__device__ void dif(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
-    int s = logn, h0 = 1 << (logn - 1);
-    while (s > 0) {
-        if (s >= 4) {
-            dif_pass<4>(A0, A1, logn, h0, tw);
-            h0 >>= 4;
-            s -= 4;
-        } else if (s == 3) {
-            dif_pass<3>(A0, A1, logn, h0, tw);
-            s = 0;
-        } else if (s == 2) {
-            dif_pass<2>(A0, A1, logn, h0, tw);
-            s = 0;
+// Forward passes from S remaining stages down (h0 = 2^(S-1)); two primes
+// split the CTA (TWO) or one prime uses all of it.
+template <bool TWO, int PR, int LOGN, int S>
+__device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
+    if constexpr (S > 0) {
+        constexpr int RLOG = S >= 4 ? 4 : S;
+        if constexpr (TWO) {
+            constexpr int half = THREADS / 2;
+            if ((int)threadIdx.x < half)
+                dif_pass_t<0, RLOG, LOGN, S - 1, half>(A0, tw.w[0], tw.wsh[0], threadIdx.x);
+            else
+                dif_pass_t<1, RLOG, LOGN, S - 1, half>(A1, tw.w[1], tw.wsh[1], threadIdx.x - half);
         } else {
-            dif_pass<1>(A0, A1, logn, h0, tw);
-            s = 0;
+            dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x);
         }
         __syncthreads();
+        dif_from<TWO, PR, LOGN, S - RLOG>(A0, A1, tw);
+    }
+}
+
+// Inverse passes from h0 = 2^LH0 up; the remainder pass (LOGN mod 4) first.
+template <bool TWO, int PR, int LOGN, int LH0>
+__device__ __forceinline__ void dit_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
+    if constexpr (LH0 < LOGN) {
+        constexpr int RLOG = (LH0 == 0 && (LOGN & 3)) ? (LOGN & 3) : 4;
+        if constexpr (TWO) {
+            constexpr int half = THREADS / 2;
+            if ((int)threadIdx.x < half)
+                dit_pass_t<0, RLOG, LOGN, LH0, half>(A0, tw.wi[0], tw.wish[0], threadIdx.x);
+            else
+                dit_pass_t<1, RLOG, LOGN, LH0, half>(A1, tw.wi[1], tw.wish[1], threadIdx.x - half);
+        } else {
+            dit_pass_t<PR, RLOG, LOGN, LH0, THREADS>(A0, tw.wi[PR], tw.wish[PR], threadIdx.x);
+        }
+        __syncthreads();
+        dit_from<TWO, PR, LOGN, LH0 + RLOG>(A0, A1, tw);
+    }
+}
+
+#define PFB_LOGN_CASES(F) \
+    F(7) F(8) F(9) F(10) F(11) F(12) F(13) F(14) F(15)
+
+__device__ void dif(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
+    switch (logn) {
+#define PFB_CASE(n)                                  \
+    case n:                                          \
+        dif_from<true, 0, n, n>(A0, A1, tw);         \
+        return;
+        PFB_LOGN_CASES(PFB_CASE)
+#undef PFB_CASE
     }
 }
 
 __device__ void dit(uint32_t *A0, uint32_t *A1, int logn, const Twiddles &tw) {
-    int s = logn, h0 = 1;
-    const int r0 = logn & 3;  // remainder pass first
-    if (r0) {
-        if (r0 == 3) dit_pass<3>(A0, A1, logn, h0, tw);
-        else if (r0 == 2) dit_pass<2>(A0, A1, logn, h0, tw);
-        else dit_pass<1>(A0, A1, logn, h0, tw);
-        h0 <<= r0;
-        s -= r0;
-        __syncthreads();
-    }
-    while (s > 0) {
-        dit_pass<4>(A0, A1, logn, h0, tw);
-        h0 <<= 4;
-        s -= 4;
-        __syncthreads();
+    switch (logn) {
+#define PFB_CASE(n)                                  \
+    case n:                                          \
+        dit_from<true, 0, n, 0>(A0, A1, tw);         \
+        return;
+        PFB_LOGN_CASES(PFB_CASE)
+#undef PFB_CASE
     }
 }
 
 // Single-prime transforms: all threads of the CTA work on prime PR.
 template <int PR>
-__device__ void dif1(uint32_t *A, int logn, const uint32_t *W, const uint32_t *Wsh) {
-    int s = logn, h0 = 1 << (logn - 1);
-    const int g0 = threadIdx.x, st = blockDim.x;
-    while (s > 0) {
-        if (s >= 4) {
-            dif_pass1<PR, 4>(A, logn, h0, W, Wsh, g0, st);
-            h0 >>= 4;
-            s -= 4;
-        } else if (s == 3) {
-            dif_pass1<PR, 3>(A, logn, h0, W, Wsh, g0, st);
-            s = 0;
-        } else if (s == 2) {
-            dif_pass1<PR, 2>(A, logn, h0, W, Wsh, g0, st);
-            s = 0;
-        } else {
-            dif_pass1<PR, 1>(A, logn, h0, W, Wsh, g0, st);
-            s = 0;
-        }
-        __syncthreads();
+__device__ void dif1(uint32_t *A, int logn, const Twiddles &tw) {
+    switch (logn) {
+#define PFB_CASE(n)                                  \
+    case n:                                          \
+        dif_from<false, PR, n, n>(A, nullptr, tw);   \
+        return;
+        PFB_LOGN_CASES(PFB_CASE)
+#undef PFB_CASE
     }
 }
 
 template <int PR>
-__device__ void dit1(uint32_t *A, int logn, const uint32_t *W, const uint32_t *Wsh) {
-    int s = logn, h0 = 1;
-    const int g0 = threadIdx.x, st = blockDim.x;
-    const int r0 = logn & 3;
-    if (r0) {
-        if (r0 == 3) dit_pass1<PR, 3>(A, logn, h0, W, Wsh, g0, st);
-        else if (r0 == 2) dit_pass1<PR, 2>(A, logn, h0, W, Wsh, g0, st);
-        else dit_pass1<PR, 1>(A, logn, h0, W, Wsh, g0, st);
-        h0 <<= r0;
-        s -= r0;
-        __syncthreads();
-    }
-    while (s > 0) {
-        dit_pass1<PR, 4>(A, logn, h0, W, Wsh, g0, st);
-        h0 <<= 4;
-        s -= 4;
-        __syncthreads();
+__device__ void dit1(uint32_t *A, int logn, const Twiddles &tw) {
+    switch (logn) {
+#define PFB_CASE(n)                                  \
+    case n:                                          \
+        dit_from<false, PR, n, 0>(A, nullptr, tw);   \
+        return;
+        PFB_LOGN_CASES(PFB_CASE)
+#undef PFB_CASE
     }
 }
 
@@ -580,7 +596,7 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     };
     if (square || (MUL && gy)) {
         load_x(X, false);
-        dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
+        dif1<0>(A, logl, tw);
         if (MUL && gy) {
             pointwise1<0, true>(A, gy, L, cc);
         } else {
@@ -590,10 +606,10 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
             }
             __syncthreads();
         }
-        dit1<0>(A, logl, tw.wi[0], tw.wish[0]);
+        dit1<0>(A, logl, tw);
         spill(L);
         load_x(X, false);
-        dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
+        dif1<1>(A, logl, tw);
         if (MUL && gy) {
             pointwise1<1, true>(A, gy + L, L, cc);
         } else {
@@ -603,7 +619,7 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
             }
             __syncthreads();
         }
-        dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
+        dit1<1>(A, logl, tw);
         carry_pass<true>(L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
         cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
@@ -615,27 +631,27 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
         load_x(X, false);
     }
     // m = T_lo * N' mod R
-    dif1<0>(A, logl, tw.w[0], tw.wsh[0]);
+    dif1<0>(A, logl, tw);
     pointwise1<0>(A, cd.nph, L, cc);
-    dit1<0>(A, logl, tw.wi[0], tw.wish[0]);
+    dit1<0>(A, logl, tw);
     spill(H);
     load_x(sp.t, true);
-    dif1<1>(A, logl, tw.w[1], tw.wsh[1]);
+    dif1<1>(A, logl, tw);
     pointwise1<1>(A, cd.nph + L, L, cc);
-    dit1<1>(A, logl, tw.wi[1], tw.wish[1]);
+    dit1<1>(A, logl, tw);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
     for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1)
-    dif1<0>(A, logl - 1, tw.w[0], tw.wsh[0]);
+    dif1<0>(A, logl - 1, tw);
     pointwise1<0>(A, cd.nh, H, cc);
-    dit1<0>(A, logl - 1, tw.wi[0], tw.wish[0]);
+    dit1<0>(A, logl - 1, tw);
     spill(H);
     for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
     __syncthreads();
-    dif1<1>(A, logl - 1, tw.w[1], tw.wsh[1]);
+    dif1<1>(A, logl - 1, tw);
     pointwise1<1>(A, cd.nh + H, H, cc);
-    dit1<1>(A, logl - 1, tw.wi[1], tw.wish[1]);
+    dit1<1>(A, logl - 1, tw);
     const unsigned long long cW = carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl - 1, cc); }, A, cs);
     unsigned long long c = carry_pass<true>(
