@@ -136,11 +136,18 @@ __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, const in
 template <bool MUL>
 __device__ __forceinline__ void mstep_t(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
                                         const JobDev &jb, const uint32_t *gy) {
-    if (cd.logl <= LOG_LCTA) {
-        mont_step<MUL>(sm, cd, square, a, tw, c_crt, gy);
-    } else {
+    static_assert(LOG_LCTA == 14 && LOG_LSEQ == 15, "length cases below");
+    switch (cd.logl) {
+#define PFB_STEP(n)                                                  \
+    case n:                                                          \
+        mont_step<MUL, n>(sm, cd, square, a, tw, c_crt, gy);        \
+        break;
+        PFB_STEP(8) PFB_STEP(9) PFB_STEP(10) PFB_STEP(11) PFB_STEP(12) PFB_STEP(13) PFB_STEP(14)
+#undef PFB_STEP
+    default: {
         const Spill sp{jb.spill_s, jb.spill_t};
-        mont_step_seq<MUL>(sm, cd, square, a, tw, c_crt, sp, gy);
+        mont_step_seq<MUL, LOG_LSEQ>(sm, cd, square, a, tw, c_crt, sp, gy);
+    }
     }
 }
 

@@ -353,9 +353,9 @@ struct CarrySmem {
 // segment of n/T consecutive positions; the carries between segments are
 // resolved by a generate/propagate scan (warp ballots, then across warps).
 template <bool PAD, class Get>
-__device__ unsigned long long carry_pass(const int n, const unsigned long long cin0, Get get, uint32_t *out,
-                                         CarrySmem &cs) {
-    const int T = blockDim.x;
+__device__ __forceinline__ unsigned long long carry_pass(const int n, const unsigned long long cin0, Get get,
+                                                         uint32_t *out, CarrySmem &cs) {
+    constexpr int T = THREADS;  // every kernel of the engine runs THREADS threads per CTA
     const int w = n >= 2 * T ? n / T : 2;  // >= 2 limbs: a carry-in (< 2^41) never overflows a segment twice
     const int na = n / w;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -495,10 +495,10 @@ struct Smem {
 // same launch.  On entry X, Y < B N with R > B^2 N (B = 4 for the strong
 // test's squarings), or X < R for a plain REDC; on exit X < 2N * a.
 // MUL = false compiles the squaring / REDC forms only (gy ignored).
-template <bool MUL = false>
+template <bool MUL, int LOGL>
 __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
                           const CrtConsts &cc, const uint32_t *gy = nullptr) {
-    const int logl = cd.logl, L = 1 << logl, H = L >> 1;
+    constexpr int logl = LOGL, L = 1 << logl, H = L >> 1;
     uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
     CarrySmem &cs = *sm.cs;
     const int tid = threadIdx.x, T = blockDim.x;
@@ -511,7 +511,7 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
             A1[pad(i)] = v;
         }
         __syncthreads();
-        dif(A0, A1, logl, tw);
+        dif_from<true, 0, LOGL, LOGL>(A0, A1, tw);
         if (MUL && gy) {
             pointwise2<true>(A0, A1, gy, gy + L, L, cc);
         } else {
@@ -523,7 +523,7 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
             }
             __syncthreads();
         }
-        dit(A0, A1, logl, tw);
+        dit_from<true, 0, LOGL, 0>(A0, A1, tw);
         // T = x^2 (or x y) as L limbs, in place over A0
         carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
         // S1 = T_lo + T_hi  -> X, carry cS
@@ -544,16 +544,16 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
         __syncthreads();
     }
     // m = T_lo * N' mod R
-    dif(A0, A1, logl, tw);
+    dif_from<true, 0, LOGL, LOGL>(A0, A1, tw);
     pointwise2(A0, A1, cd.nph, cd.nph + L, L, cc);
-    dit(A0, A1, logl, tw);
+    dit_from<true, 0, LOGL, 0>(A0, A1, tw);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
     for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1): cyclic product of length H
-    dif(A0, A1, logl - 1, tw);
+    dif_from<true, 0, LOGL - 1, LOGL - 1>(A0, A1, tw);
     pointwise2(A0, A1, cd.nh, cd.nh + H, H, cc);
-    dit(A0, A1, logl - 1, tw);
+    dit_from<true, 0, LOGL - 1, 0>(A0, A1, tw);
     const unsigned long long cW =
         carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl - 1, cc); }, A0, cs);
     // U = S1 + W (mod R - 1); S1 = X (square = false: S1 = x itself)
@@ -578,10 +578,10 @@ __device__ __forceinline__ uint32_t ldg_spill(const uint32_t *p) { return __ldcg
 // mont_step for transforms too long for both primes to sit in shared memory
 // (L = 2^15): the p1 spectrum makes a round trip through global memory (L2).
 // Same arithmetic and result as mont_step; sm.A1 is unused.
-template <bool MUL = false>
+template <bool MUL, int LOGL>
 __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
                               const CrtConsts &cc, const Spill &sp, const uint32_t *gy = nullptr) {
-    const int logl = cd.logl, L = 1 << logl, H = L >> 1;
+    constexpr int logl = LOGL, L = 1 << logl, H = L >> 1;
     uint32_t *A = sm.A0, *X = sm.X;
     CarrySmem &cs = *sm.cs;
     const int tid = threadIdx.x, T = blockDim.x;
@@ -596,7 +596,7 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     };
     if (square || (MUL && gy)) {
         load_x(X, false);
-        dif1<0>(A, logl, tw);
+        dif_from<false, 0, LOGL, LOGL>(A, nullptr, tw);
         if (MUL && gy) {
             pointwise1<0, true>(A, gy, L, cc);
         } else {
@@ -606,10 +606,10 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
             }
             __syncthreads();
         }
-        dit1<0>(A, logl, tw);
+        dit_from<false, 0, LOGL, 0>(A, nullptr, tw);
         spill(L);
         load_x(X, false);
-        dif1<1>(A, logl, tw);
+        dif_from<false, 1, LOGL, LOGL>(A, nullptr, tw);
         if (MUL && gy) {
             pointwise1<1, true>(A, gy + L, L, cc);
         } else {
@@ -619,7 +619,7 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
             }
             __syncthreads();
         }
-        dit1<1>(A, logl, tw);
+        dit_from<false, 1, LOGL, 0>(A, nullptr, tw);
         carry_pass<true>(L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
         cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
@@ -631,27 +631,27 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
         load_x(X, false);
     }
     // m = T_lo * N' mod R
-    dif1<0>(A, logl, tw);
+    dif_from<false, 0, LOGL, LOGL>(A, nullptr, tw);
     pointwise1<0>(A, cd.nph, L, cc);
-    dit1<0>(A, logl, tw);
+    dit_from<false, 0, LOGL, 0>(A, nullptr, tw);
     spill(H);
     load_x(sp.t, true);
-    dif1<1>(A, logl, tw);
+    dif_from<false, 1, LOGL, LOGL>(A, nullptr, tw);
     pointwise1<1>(A, cd.nph + L, L, cc);
-    dit1<1>(A, logl, tw);
+    dit_from<false, 1, LOGL, 0>(A, nullptr, tw);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
     for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1)
-    dif1<0>(A, logl - 1, tw);
+    dif_from<false, 0, LOGL - 1, LOGL - 1>(A, nullptr, tw);
     pointwise1<0>(A, cd.nh, H, cc);
-    dit1<0>(A, logl - 1, tw);
+    dit_from<false, 0, LOGL - 1, 0>(A, nullptr, tw);
     spill(H);
     for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
     __syncthreads();
-    dif1<1>(A, logl - 1, tw);
+    dif_from<false, 1, LOGL - 1, LOGL - 1>(A, nullptr, tw);
     pointwise1<1>(A, cd.nh + H, H, cc);
-    dit1<1>(A, logl - 1, tw);
+    dit_from<false, 1, LOGL - 1, 0>(A, nullptr, tw);
     const unsigned long long cW = carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl - 1, cc); }, A, cs);
     unsigned long long c = carry_pass<true>(
