@@ -133,6 +133,36 @@ def ref_trial_div_cpu(primes: np.ndarray, a: int, b: int, c: int,
     return bits
 
 
+class _SieveTable(C.Structure):
+    # sieve_table.h: { sieve_entry_t *entries; int n; uint32_t *flat_data; size_t flat_size; int shared; }
+    _fields_ = [("entries", C.c_void_p), ("n", C.c_int), ("flat_data", C.c_void_p),
+                ("flat_size", C.c_size_t), ("shared", C.c_int)]
+
+
+def ref_phase0_masks(small_primes: np.ndarray, abc) -> np.ndarray:
+    """The reference's own Phase 0: sieve_table_build over small_primes, then
+    sieve_apply per triple; returns [len(abc), 313] u32 masks.  Builds the
+    whole table (4 GB for the primes below 1e4)."""
+    L = C.CDLL(os.path.join(REF_DIR, "libref_phase0.so"))
+    L.sieve_table_build.argtypes = [C.POINTER(_SieveTable), C.c_int, C.POINTER(_PrimeList)]
+    L.sieve_table_build.restype = C.c_int
+    L.sieve_apply.argtypes = [C.POINTER(_SieveTable), C.c_longlong, C.c_longlong, C.c_longlong,
+                              C.POINTER(C.c_uint32)]
+    L.sieve_apply.restype = None
+    L.sieve_table_free.argtypes = [C.POINTER(_SieveTable)]
+    L.sieve_table_free.restype = None
+    small_primes = np.ascontiguousarray(small_primes, dtype=np.uint32)
+    pl = _PrimeList(_ptr(small_primes, C.c_uint32), len(small_primes))
+    st = _SieveTable()
+    if L.sieve_table_build(C.byref(st), 0, C.byref(pl)) != 0:
+        raise RuntimeError("sieve_table_build failed")
+    out = np.zeros((len(abc), 313), dtype=np.uint32)
+    for i, (a, b, c) in enumerate(abc):
+        L.sieve_apply(C.byref(st), a, b, c, _ptr(out[i], C.c_uint32))
+    L.sieve_table_free(C.byref(st))
+    return out
+
+
 def ref_miller_rabin_test(a: int, b: int, c: int, k: int, j: int) -> int:
     """The reference's own miller_rabin_test (GMP BPSW on N, then rev(N))."""
     global _ref_mr

@@ -614,3 +614,66 @@ def pipeline_run(sieve: "Sieve", engine: "MillerRabin", abc, K: int, pre_mask: O
                               C.byref(st)), "pfb_pipeline_run")
     recs = [(r.a, r.b, r.c, r.k, r.j, r.result) for r in out[:n_out.value]]
     return recs, {f: getattr(st, f) for f, _ in PipelineStats._fields_}
+
+
+# ------------------------------------------------------------------ phase 0 ---
+
+def _phase0_lib():
+    L = lib()
+    if not hasattr(L, "_phase0_ready"):
+        vp = C.c_void_p
+        L.pfb_phase0_create.argtypes = [C.POINTER(vp), C.POINTER(C.c_uint32), C.c_uint32, C.c_int]
+        L.pfb_phase0_create.restype = C.c_int
+        L.pfb_phase0_apply.argtypes = [vp, C.POINTER(C.c_longlong), C.c_int, vp, C.c_uint, vp]
+        L.pfb_phase0_apply.restype = C.c_int
+        L.pfb_phase0_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_longlong), C.POINTER(C.c_size_t),
+                                      C.POINTER(C.c_double)]
+        L.pfb_phase0_info.restype = C.c_int
+        L.pfb_phase0_destroy.argtypes = [vp]
+        L.pfb_phase0_destroy.restype = None
+        L._phase0_ready = True
+    return L
+
+
+class Phase0:
+    """The Phase-0 periodic table in device memory (pfb_phase0_* C ABI)."""
+
+    def __init__(self, small_primes: np.ndarray, device: int = 0):
+        small_primes = np.ascontiguousarray(small_primes, dtype=np.uint32)
+        h = C.c_void_p()
+        _check(_phase0_lib().pfb_phase0_create(C.byref(h), _u32(small_primes), len(small_primes), device),
+               "pfb_phase0_create")
+        self._h = h
+
+    def info(self) -> dict:
+        n, m, b, s = C.c_int(0), C.c_longlong(0), C.c_size_t(0), C.c_double(0)
+        _check(_phase0_lib().pfb_phase0_info(self._h, C.byref(n), C.byref(m), C.byref(b), C.byref(s)),
+               "pfb_phase0_info")
+        return {"primes": n.value, "masks": m.value, "table_bytes": b.value, "build_seconds": s.value}
+
+    def apply(self, abc, masks=None, or_in: bool = False, stream: int = 0):
+        """313-word masks of the triples: into a host array (returned) or a
+        device buffer (asynchronous on stream)."""
+        flat, pabc, n = _abc_array(abc)
+        flags = SIEVE_OR if or_in else 0
+        if masks is None or isinstance(masks, np.ndarray):
+            if masks is None:
+                masks = np.zeros((n, 313), dtype=np.uint32)
+            masks = np.ascontiguousarray(masks, dtype=np.uint32)
+            _check(_phase0_lib().pfb_phase0_apply(self._h, pabc, n, masks.ctypes.data, flags | SIEVE_MASK_HOST,
+                                                  None), "pfb_phase0_apply")
+            return masks
+        _check(_phase0_lib().pfb_phase0_apply(self._h, pabc, n, _dptr(masks), flags, stream or None),
+               "pfb_phase0_apply")
+        return masks
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _phase0_lib().pfb_phase0_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
