@@ -677,3 +677,56 @@ class Phase0:
             self.close()
         except Exception:
             pass
+
+
+# ------------------------------------------------------------------ formats ---
+
+class Candidate(C.Structure):
+    """pfb_candidate_t"""
+    _fields_ = [("a", C.c_longlong), ("b", C.c_longlong), ("c", C.c_longlong), ("k", C.c_int), ("j", C.c_int)]
+
+
+def _formats_lib():
+    L = lib()
+    if not hasattr(L, "_formats_ready"):
+        L.pfb_read_candidates.argtypes = [C.c_char_p, C.POINTER(Candidate), C.c_longlong]
+        L.pfb_read_candidates.restype = C.c_longlong
+        for fn in (L.pfb_write_phase1, L.pfb_write_phase2):
+            fn.argtypes = [C.c_char_p, C.POINTER(Phase2Record), C.c_longlong, C.c_int]
+            fn.restype = C.c_longlong
+        L._formats_ready = True
+    return L
+
+
+def read_candidates(path: str):
+    """[(a, b, c, k, j), ...] of a candidate file (pfb_read_candidates)."""
+    L = _formats_lib()
+    n = L.pfb_read_candidates(path.encode(), None, 0)
+    if n < 0:
+        raise PfbError(int(n), "pfb_read_candidates")
+    out = (Candidate * max(1, n))()
+    L.pfb_read_candidates(path.encode(), out, n)
+    return [(r.a, r.b, r.c, r.k, r.j) for r in out[:n]]
+
+
+def _records(recs):
+    arr = (Phase2Record * max(1, len(recs)))()
+    for i, r in enumerate(recs):
+        arr[i] = Phase2Record(*(list(r[:5]) + [r[5] if len(r) > 5 else 0]))
+    return arr
+
+
+def write_phase1(path: str, recs, append: bool = False) -> int:
+    """Survivor lines "a=.. b=.. c=.. k=.. j=.." (pfb_write_phase1)."""
+    n = _formats_lib().pfb_write_phase1(path.encode(), _records(recs), len(recs), int(append))
+    if n < 0:
+        raise PfbError(int(n), "pfb_write_phase1")
+    return int(n)
+
+
+def write_phase2(path: str, recs, append: bool = False) -> int:
+    """Hit lines for result 2 / 3 records (pfb_write_phase2)."""
+    n = _formats_lib().pfb_write_phase2(path.encode(), _records(recs), len(recs), int(append))
+    if n < 0:
+        raise PfbError(int(n), "pfb_write_phase2")
+    return int(n)
