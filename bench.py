@@ -298,6 +298,23 @@ def main():
     # compulsory HBM bytes of one triple: the prime list read once, the mask written once
     sieve_bytes = 4 * len(primes) + pfb200.mask_bytes(K)
     sieve_gbs = sieve_bytes * ntr * len(times) / max_over_ranks(sum(times)) / 1e9
+    # Phase-0 periodic table (primes below 1e4) built on the device, applied per triple
+    p0 = pfb200.Phase0(primes[primes < 10000], dev)
+    p0_info = p0.info()
+    p0_abc = sieve_triples(4096)
+    d_p0 = torch.zeros(len(p0_abc) * 313, dtype=torch.int32, device="cuda")
+    with torch.cuda.stream(stream):
+        p0.apply(p0_abc, d_p0, stream=stream.cuda_stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        p0.apply(p0_abc, d_p0, stream=stream.cuda_stream)
+        e1.record(stream)
+        stream.synchronize()
+    phase0 = {"build_s": p0_info["build_seconds"], "masks": p0_info["masks"], "primes": p0_info["primes"],
+              "table_gb": p0_info["table_bytes"] / 1e9,
+              "apply_triples_per_s": len(p0_abc) / (e0.elapsed_time(e1) / 1e3)}
+    p0.close()
+    del d_p0
     t = pfb200.GpuTiming()
     pfb200.trial_div_gpu(primes, *abc1, None, t)
     t0 = time.perf_counter()
@@ -493,6 +510,7 @@ def main():
         "served_over_plain": tests_s / world / plain_tests_s,
         "uneven": uneven,
         "autotune": autotune,
+        "phase0": phase0,
         "sieve": {"value": sieve_pairs_s, "unit": "pairs/s", "K": K, "triples_per_step": ntr,
                   "ms_per_triple": 1e3 / (sieve_pairs_s / world / (K * K)),
                   "hbm_compulsory_gbs": sieve_gbs, "hbm_compulsory_bytes_per_triple": sieve_bytes,
