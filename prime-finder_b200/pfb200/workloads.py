@@ -8,7 +8,8 @@ make the golden fixtures, so that both draw exactly the same candidates.
                         (50000, 30000, 100): with N and rev(N), the 256
                         50 000-digit numbers of the uniform batch
   sieve_triples         (a,b,c) of the wide-grid sieve runs: a in
-                        [50000, 50063]; per a, c = 100 and b = c+1, c+1+997, ...
+                        [50000, 50063], c = 100, 101, ..., b = c+1, c+1+997, ...
+                        up to a-1
   uneven_tuples         512 (a,b,c,k,j,rev) with splitmix64(seed=2):
                         a ~ U[50000, 100000], c ~ U[100, 1000], b ~ U[c+1, a-1],
                         k, j ~ U[1, 9999], rev ~ U{0,1}; a tuple is drawn again
@@ -42,16 +43,21 @@ def uniform_batch_pairs(survivors, n: int = 128, seed: int = 1):
 
 
 def sieve_triples(n: int):
-    """The first n triples, a-major over b."""
+    """The first n triples: c = 100, 101, ...; per c, b = c+1, c+1+997, ...
+    (b <= a-1); per b, a = 50000 .. 50063."""
     out = []
-    i = 0
+    c = 100
     while len(out) < n:
-        a = 50000 + (i % 64)
-        c = 100
-        b = c + 1 + 997 * (i // 64)
-        if b <= a - 1:
-            out.append((a, b, c))
-        i += 1
+        bi = 0
+        while len(out) < n:
+            b = c + 1 + 997 * bi
+            if b > 50063 - 1:
+                break
+            for a in range(50000, 50064):
+                if b <= a - 1 and len(out) < n:
+                    out.append((a, b, c))
+            bi += 1
+        c += 1
     return out
 
 

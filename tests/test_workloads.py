@@ -46,3 +46,10 @@ def test_serving_draw_constraints():
     for _ in range(50):
         a, b, c, k, j, rev = W.serving_draw(rng)
         assert a - b - len(str(k)) >= 2 and b - c > len(str(j))
+
+
+def test_sieve_triples_continue_past_the_first_c():
+    t = W.sieve_triples(5000)
+    assert len(t) == 5000 and len(set(t)) == 5000
+    assert all(50000 <= a <= 50063 and c < b <= a - 1 for a, b, c in t)
+    assert t[3264] == (50000, 102, 101)
