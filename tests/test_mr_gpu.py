@@ -242,3 +242,15 @@ def test_autotune_picks_a_timed_pair_and_results_hold(mr):
     ver, res = mr.test(Ns, 2)
     for N, v, r in zip(Ns, ver, res):
         assert r == oracle.strong_residue(N, 2)[1] and v == oracle.strong_test(N, 2)
+
+
+def test_small_moduli_long_s_and_bases_multiple_of_n(mr):
+    """Tiny moduli, s up to 16 (Fermat primes), Mersenne primes with s = 1,
+    and bases that are multiples of N, against GMP's strong test."""
+    Ns = [3, 5, 7, 11, 13, 17, 257, 65537, 641 * 6700417, (1 << 61) - 1, (1 << 127) - 1, 2**64 + 13]
+    for base in (2, 3, 7, 17, 257, 65535):
+        ver, res = mr.test(Ns, base)
+        for N, v, r in zip(Ns, ver, res):
+            s, rg = oracle.strong_residue(N, base)
+            assert r == rg, (N, base)
+            assert v == oracle.strong_test(N, base), (N, base)
