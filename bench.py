@@ -14,7 +14,7 @@ Beside it the line reports:
                host set-up, H2D, every squaring, verdict + residue D2H
   plain        the one-candidate-per-call form on the same GPU
   sieve        K = 9999 grid pairs/s over the (a,b,c) triples of the
-               config-2 enumeration, and the drop-in 100 x 100 call
+               wide-grid triple enumeration, and the drop-in 100 x 100 call
   roofline     INT32 multiplies of the reference's squaring structure
                (6 length-L transforms + 3 pointwise products, 2 primes, 3
                multiplies per modmul, L = 32768 at 50 000 digits) per second,
@@ -41,6 +41,9 @@ from pfb200 import replicas  # noqa: E402
 from pfb200.workloads import serving_draw, sieve_triples, uneven_tuples, uniform_batch_pairs  # noqa: E402
 
 SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference count)
+METRIC = "MR base-2 tests/s, uniform batch of 256 x 50 000-digit candidates, served/batched"
+WORKLOAD = ("uniform MR batch: 256 x 50 000-digit N/rev(N), (k,j) from the (50000,30000,100) sieve "
+            "survivors, splitmix64 seed 1")
 PERSIST_LAUNCH_DRAM_BYTES = 137718528 + 21966848  # dram__bytes_read.sum + dram__bytes_write.sum
 
 
@@ -196,7 +199,7 @@ def main():
     ap.add_argument("--no-uneven", action="store_true", help="skip the 512-candidate uneven batch")
     ap.add_argument("--sieve-triples", type=int, default=4)
     ap.add_argument("--serve-secs", type=float, default=0.0,
-                    help="also run the serving loop (Poisson arrivals, config 5 shapes) this long")
+                    help="also run the serving loop (Poisson arrivals of 50k-100k-digit requests) this long")
     ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
     args = ap.parse_args()
 
@@ -207,7 +210,7 @@ def main():
         if rank != 0:
             return
         import json as _j
-        g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_config1.json")))
+        g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_50000_30000_100.json")))
         pairs = [tuple(x) for x in g["survivors_99"]]
         t0 = time.perf_counter()
         steps = []
@@ -217,11 +220,11 @@ def main():
         v = statistics.mean(vals)
         last = steps[-1]
         print(json.dumps({
-            "impl": "reference", "metric": "MR base-2 tests/s, 50 000-digit batch (config 3)",
+            "impl": "reference", "metric": METRIC,
             "value": v, "unit": "tests/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * (time.perf_counter() - t0) / max(1, len(steps)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {"workload": "uniform MR batch: 256 x 50 000-digit N/rev(N) of (50000,30000,100) survivors"},
+            "config": {"workload": WORKLOAD, "candidates": 256, "parallelism": "replicas"},
             "cpu_baseline": {"kind": last["kind"], "cores": last["cores"], "sample": last["sample"], "value": v,
                              "unit": "tests/s"},
             "e2e": {"value": v, "unit": "tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
@@ -232,7 +235,7 @@ def main():
     cpu_sieve = None
     if rank == 0 and not args.no_cpu:
         import json as _j
-        g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_config1.json")))
+        g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_50000_30000_100.json")))
         pairs = [tuple(x) for x in g["survivors_99"]]
         cpu = cpu_mr_baseline(uniform_batch_pairs(pairs), abc1, sample_bits=4096)
         cpu_sieve = cpu_sieve_baseline()
@@ -498,13 +501,11 @@ def main():
     if rank != 0:
         return
     line = {
-        "metric": "MR base-2 tests/s, 50 000-digit batch (config 3), served/batched",
+        "metric": METRIC,
         "value": tests_s, "unit": "tests/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u32", "data": "synthetic",
-        "config": {"workload": "uniform MR batch: 256 x 50 000-digit N/rev(N), (k,j) from the "
-                               "(50000,30000,100) sieve survivors, splitmix64 seed 1",
-                   "candidates": n, "squarings_per_step": chunk, "squarings_per_test": sq_per_test,
+        "config": {"workload": WORKLOAD, "candidates": n, "squarings_per_step": chunk, "squarings_per_test": sq_per_test,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
         "plain": {"value": plain_tests_s, "unit": "tests/s", "form": "one candidate per call"},
         "served_over_plain": tests_s / world / plain_tests_s,

@@ -6,7 +6,7 @@ into oracle/_ref/libref_sieve.so from the reference sources) and writes:
   sieve_ref_kat.json   - 313-word masks for the prime list of tests/test_gpu.c
                          (3..97) at the (a,b,c) of tests/test_gpu.c:169-172 and
                          tests/test_sieve.c:78-80
-  sieve_config1.json   - the 100 x 100 mask at (a,b,c) = (50000, 30000, 100)
+  sieve_50000_30000_100.json   - the 100 x 100 mask at (a,b,c) = (50000, 30000, 100)
                          over every odd prime below 1e8, with its survivors
 
 Usage:  python tests/golden/make_golden.py          (needs oracle/_ref built)
@@ -53,13 +53,13 @@ def main():
     bits = oracle.ref_trial_div_cpu(P, a, b, c)
     surv = survivors(bits)
     sub = [s for s in surv if s[0] <= 99 and s[1] <= 99]
-    with open(os.path.join(HERE, "sieve_config1.json"), "w") as f:
+    with open(os.path.join(HERE, "sieve_50000_30000_100.json"), "w") as f:
         json.dump({"source": "reference trial_div_cpu.c via oracle/_ref/libref_sieve.so",
                    "primes": "odd primes below 1e8 (%d)" % len(P), "n_primes": int(len(P)),
                    "abc": [a, b, c], "words_hex": words_hex(bits),
                    "n_survivors_100": len(surv), "n_survivors_99": len(sub),
                    "survivors_99": sub}, f, indent=1)
-    print("wrote", len(kat), "KAT cases;", len(surv), "config-1 survivors (", len(sub), "on 99x99 )")
+    print("wrote", len(kat), "KAT cases;", len(surv), "(50000,30000,100) survivors (", len(sub), "on 99x99 )")
 
 
 if __name__ == "__main__":

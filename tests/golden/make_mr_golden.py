@@ -5,17 +5,20 @@ oracle/mr_oracle.c), the base-2 strong-test residue r = 2^d mod N
 (N - 1 = 2^s d) and the verdicts, and stores a SHA-256 of r (little-endian
 16-bit limbs, ceil(bits(N)/16) of them) plus its low 64 bits:
 
-  mr_config1.json  N and rev(N) of the first 16 (k,j) survivors of the
-                   (50000, 30000, 100) sieve (the reference's own
-                   miller_rabin_test verdicts are stored beside them)
-  mr_config3.json  N and rev(N) of every survivor (k,j <= 99) of that sieve:
-                   the candidates the 256-number uniform batch draws from
-  mr_config4.json  the first 32 of the 512 uneven-batch tuples
-                   (pfb200.workloads.uneven_tuples: 50 000 - 100 000 digits)
+  mr_50k_first16.json     (first16) N and rev(N) of the first 16 (k,j)
+                          survivors of the (50000, 30000, 100) sieve (the
+                          reference's own miller_rabin_test verdicts are
+                          stored beside them)
+  mr_50k_survivors.json   (survivors) N and rev(N) of every survivor
+                          (k,j <= 99) of that sieve: the candidates the
+                          256-number uniform batch draws from
+  mr_uneven_first32.json  (uneven) the first 32 of the 512 uneven-batch
+                          tuples (pfb200.workloads.uneven_tuples: 50 000 -
+                          100 000 digits)
 
 Each 50 000-digit powm takes minutes of one core; the script runs a process
 pool (spawn) over all cores.  Usage:
-  python tests/golden/make_mr_golden.py config1|config3|config4
+  python tests/golden/make_mr_golden.py first16|survivors|uneven
 """
 import hashlib
 import json
@@ -47,29 +50,30 @@ def residue_record(args):
 
 
 def main():
-    which = sys.argv[1] if len(sys.argv) > 1 else "config1"
-    sv = json.load(open(os.path.join(HERE, "sieve_config1.json")))
+    which = sys.argv[1] if len(sys.argv) > 1 else "first16"
+    sv = json.load(open(os.path.join(HERE, "sieve_50000_30000_100.json")))
     a, b, c = sv["abc"]
     pairs = [tuple(x) for x in sv["survivors_99"]]
-    if which == "config1":
+    if which == "first16":
         pairs = pairs[:16]
     jobs = [(a, b, c, k, j, rev) for (k, j) in pairs for rev in (False, True)]
-    if which == "config4":
+    if which == "uneven":
         from pfb200.workloads import uneven_tuples
         jobs = uneven_tuples(512)[:32]
     ctx = mp.get_context("spawn")
     with ctx.Pool(os.cpu_count()) as pool:
         recs = pool.map(residue_record, jobs, chunksize=1)
     out = {"source": "GMP 6.3 mpz_powm via oracle/mr_oracle.c", "base": 2, "records": recs}
-    if which != "config4":
+    if which != "uneven":
         out["abc"] = [a, b, c]
-    if which == "config1":
+    if which == "first16":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
         import oracle
         if oracle.ref_available():
             out["ref_miller_rabin_test"] = {"%d,%d" % p: oracle.ref_miller_rabin_test(a, b, c, *p)
                                             for p in pairs}
-    with open(os.path.join(HERE, "mr_%s.json" % which), "w") as f:
+    names = {"first16": "mr_50k_first16.json", "survivors": "mr_50k_survivors.json", "uneven": "mr_uneven_first32.json"}
+    with open(os.path.join(HERE, names[which]), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", len(recs), "records")
 

@@ -154,10 +154,10 @@ def _golden(name):
     return json.load(open(path))
 
 
-def test_config1_full_size_residues(mr):
+def test_first16_survivors_full_size_residues(mr):
     """50 000-digit N and rev(N) of the first 16 sieve survivors: residues
     2^d mod N must hash to the GMP values and verdicts match the reference."""
-    g = _golden("mr_config1.json")
+    g = _golden("mr_50k_first16.json")
     recs = g["records"]
     Ns = [oracle.build_candidate(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs]
     ver, res = mr.test(Ns, 2)
@@ -211,7 +211,7 @@ def _check_records(mr, recs):
 def test_uniform_batch_every_candidate_residue(mr):
     """Every number the 256-candidate 50 000-digit batch draws from (N and
     rev(N) of all 107 survivors): residues hash to GMP's, verdicts match."""
-    g = _golden("mr_config3.json")
+    g = _golden("mr_50k_survivors.json")
     assert len(g["records"]) == 214
     _check_records(mr, g["records"])
 
@@ -220,7 +220,7 @@ def test_uneven_batch_subset_residues(mr):
     """The first 32 uneven-batch candidates (50 000 - 100 000 digits, both
     transform lengths in one batch) against GMP."""
     from pfb200.workloads import uneven_tuples
-    g = _golden("mr_config4.json")
+    g = _golden("mr_uneven_first32.json")
     recs = g["records"]
     assert [(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs] == uneven_tuples(512)[:32]
     _check_records(mr, recs)

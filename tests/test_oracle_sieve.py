@@ -63,8 +63,8 @@ def test_negative_rev_exponents():
                 oracle.sieve_brute(p, a, b, c, 120)).all()
 
 
-def test_config1_golden_against_restatement():
-    g = json.load(open(os.path.join(GOLD, "sieve_config1.json")))
+def test_50000_30000_100_golden_against_restatement():
+    g = json.load(open(os.path.join(GOLD, "sieve_50000_30000_100.json")))
     P = primes_below(100_000_000)
     assert len(P) == g["n_primes"] == 5761454
     a, b, c = g["abc"]

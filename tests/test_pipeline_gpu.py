@@ -82,11 +82,11 @@ def test_pipeline_pre_mask_and_capacity(engines):
     assert ei.value.code == -4
 
 
-def test_pipeline_config1_corner(primes_1e8):
+def test_pipeline_50000_30000_100_corner(primes_1e8):
     """(50000, 30000, 100) on the 20 x 20 corner with every prime below 1e8:
     the survivors are the reference's, and every 50 000-digit N is composite
     (the reference's miller_rabin_test returns 0 for all of them)."""
-    g = json.load(open(os.path.join(GOLD, "sieve_config1.json")))
+    g = json.load(open(os.path.join(GOLD, "sieve_50000_30000_100.json")))
     sv = pfb200.Sieve(primes_1e8)
     mr = pfb200.MillerRabin(0)
     recs, st = pfb200.pipeline_run(sv, mr, [tuple(g["abc"])], 20)

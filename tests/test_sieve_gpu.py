@@ -58,8 +58,8 @@ def test_drop_in_determinism_and_or_semantics(torch_cuda):
     assert t.kernel >= 0.0 and t.upload >= 0.0 and t.download >= 0.0
 
 
-def test_drop_in_config1_golden(torch_cuda, primes_1e8):
-    g = json.load(open(os.path.join(GOLD, "sieve_config1.json")))
+def test_drop_in_50000_30000_100_golden(torch_cuda, primes_1e8):
+    g = json.load(open(os.path.join(GOLD, "sieve_50000_30000_100.json")))
     a, b, c = g["abc"]
     bits = pfb200.trial_div_gpu(primes_1e8, a, b, c)
     assert (bits == _words(g["words_hex"])).all()
@@ -90,7 +90,7 @@ def test_wide_grid_vs_oracle_small_primes(torch_cuda, K):
 
 
 def test_wide_grid_k9999_vs_oracle(torch_cuda):
-    # config-2 style triples (c from 100, b = c+1 + 997*i) with primes < 2e6
+    # triples of the wide-grid enumeration (c from 100, b = c+1 + 997 i) with primes < 2e6
     P = primes_below(2_000_000)
     abc = [(50000, 101, 100), (50001, 101 + 997 * 7, 100), (50063, 101 + 997 * 40, 101)]
     s = pfb200.Sieve(P)
@@ -104,7 +104,7 @@ def test_wide_grid_k9999_vs_oracle(torch_cuda):
 
 def test_k9999_full_primes_subgrid_matches_reference(torch_cuda, primes_1e8):
     # (k,j) <= 100 of a K = 9999 run must equal the reference's 100 x 100 grid.
-    g = json.load(open(os.path.join(GOLD, "sieve_config1.json")))
+    g = json.load(open(os.path.join(GOLD, "sieve_50000_30000_100.json")))
     a, b, c = g["abc"]
     s = pfb200.Sieve(primes_1e8)
     m = pfb200.unpack_mask(s.run([(a, b, c)], 9999), 9999)
