@@ -573,6 +573,17 @@ struct Spill {
     uint32_t *t;   // H words: T mod R, then m
 };
 
+// Layout of the spilled prime-1 coefficients of an n-point product, n >= 2T:
+// the CRT's carry pass gives thread t the w = n/T consecutive positions
+// t w .. t w + w - 1, so position t w + q is stored at q T + t and the
+// pass's q-th reads of all threads are one coalesced line.
+template <int N>
+__device__ __forceinline__ int spill_slot(int i) {
+    constexpr int W = N / THREADS;
+    static_assert(N >= 2 * THREADS && W * THREADS == N, "carry-pass segments");
+    return (i % W) * THREADS + i / W;
+}
+
 __device__ __forceinline__ uint32_t ldg_spill(const uint32_t *p) { return __ldcg(p); }
 
 // mont_step for transforms too long for both primes to sit in shared memory
@@ -584,14 +595,22 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     constexpr int logl = LOGL, L = 1 << logl, H = L >> 1;
     uint32_t *A = sm.A0, *X = sm.X;
     CarrySmem &cs = *sm.cs;
-    const int tid = threadIdx.x, T = blockDim.x;
+    const int tid = threadIdx.x;
+    constexpr int T = THREADS;
     unsigned long long cS = 0;
     auto load_x = [&](const uint32_t *src, bool from_global) {
         for (int i = tid; i < L; i += T) A[pad(i)] = i < H ? (from_global ? ldg_spill(src + i) : src[pad(i)]) : 0u;
         __syncthreads();
     };
-    auto spill = [&](int n) {
-        for (int i = tid; i < n; i += T) sp.s[i] = A[pad(i)];
+    // coalesced writes: slot j holds position (j mod T) w + j / T
+    auto spill_L = [&]() {
+        constexpr int W = L / T;
+        for (int j = tid; j < L; j += T) sp.s[j] = A[pad((j % T) * W + j / T)];
+        __syncthreads();
+    };
+    auto spill_H = [&]() {
+        constexpr int W = H / T;
+        for (int j = tid; j < H; j += T) sp.s[j] = A[pad((j % T) * W + j / T)];
         __syncthreads();
     };
     if (square || (MUL && gy)) {
@@ -607,7 +626,7 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
             __syncthreads();
         }
         dit_from<false, 0, LOGL, 0>(A, nullptr, tw);
-        spill(L);
+        spill_L();
         load_x(X, false);
         dif_from<false, 1, LOGL, LOGL>(A, nullptr, tw);
         if (MUL && gy) {
@@ -620,7 +639,8 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
             __syncthreads();
         }
         dit_from<false, 1, LOGL, 0>(A, nullptr, tw);
-        carry_pass<true>(L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
+        carry_pass<true>(
+            L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<L>(i)), A[pad(i)], logl, cc); }, A, cs);
         cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
         for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
@@ -634,26 +654,27 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     dif_from<false, 0, LOGL, LOGL>(A, nullptr, tw);
     pointwise1<0>(A, cd.nph, L, cc);
     dit_from<false, 0, LOGL, 0>(A, nullptr, tw);
-    spill(H);
+    spill_H();
     load_x(sp.t, true);
     dif_from<false, 1, LOGL, LOGL>(A, nullptr, tw);
     pointwise1<1>(A, cd.nph + L, L, cc);
     dit_from<false, 1, LOGL, 0>(A, nullptr, tw);
-    carry_pass<true>(H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl, cc); }, A, cs);
+    carry_pass<true>(
+        H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl, cc); }, A, cs);
     for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1)
     dif_from<false, 0, LOGL - 1, LOGL - 1>(A, nullptr, tw);
     pointwise1<0>(A, cd.nh, H, cc);
     dit_from<false, 0, LOGL - 1, 0>(A, nullptr, tw);
-    spill(H);
+    spill_H();
     for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
     __syncthreads();
     dif_from<false, 1, LOGL - 1, LOGL - 1>(A, nullptr, tw);
     pointwise1<1>(A, cd.nh + H, H, cc);
     dit_from<false, 1, LOGL - 1, 0>(A, nullptr, tw);
     const unsigned long long cW = carry_pass<true>(
-        H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + i), A[pad(i)], logl - 1, cc); }, A, cs);
+        H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl - 1, cc); }, A, cs);
     unsigned long long c = carry_pass<true>(
         H, cS + cW, [&](int i) { return (unsigned long long)X[pad(i)] + A[pad(i)]; }, X, cs);
     while (c) c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
