@@ -7,9 +7,10 @@ baseline.  The product (``prime-finder_b200``) never imports it.
 Two families of libraries are loaded:
 
 * ``liboracle.so`` - our C restatements (``sieve_oracle.c``, ``mr_oracle.c``).
-* ``_ref/libref_sieve.so`` / ``_ref/libref_mr.so`` - the reference's own
-  ``trial_div_cpu.c``, ``prime_list.c`` and ``miller_rabin.c``, compiled
-  unmodified by ``oracle/Makefile``.
+* ``_ref/libref_sieve.so`` / ``_ref/libref_mr.so`` / ``_ref/libref_phase0.so``
+  - the reference's own ``trial_div_cpu.c``, ``prime_list.c``,
+  ``miller_rabin.c``, ``sieve_table.c`` and ``sieve.c``, compiled unmodified
+  by ``oracle/Makefile``.
 """
 from __future__ import annotations
 
