@@ -44,7 +44,7 @@ SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference coun
 METRIC = "MR base-2 tests/s, uniform batch of 256 x 50 000-digit candidates, served/batched"
 WORKLOAD = ("uniform MR batch: 256 x 50 000-digit N/rev(N), (k,j) from the (50000,30000,100) sieve "
             "survivors, splitmix64 seed 1")
-PERSIST_LAUNCH_DRAM_BYTES = 137718528 + 21966848  # dram__bytes_read.sum + dram__bytes_write.sum
+PERSIST_LAUNCH_DRAM_BYTES = 517586944 + 219800832  # dram__bytes_read.sum + dram__bytes_write.sum
 
 
 def ref_modmuls_per_squaring(digits: int) -> int:
