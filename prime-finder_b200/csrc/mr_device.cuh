@@ -252,9 +252,9 @@ __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint3
 
 // Forward passes from S remaining stages down (h0 = 2^(S-1)); two primes
 // split the CTA (TWO) or one prime uses all of it.
-template <bool TWO, int PR, int LOGN, int S>
+template <bool TWO, int PR, int LOGN, int S, int STOP = 0>
 __device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
-    if constexpr (S > 0) {
+    if constexpr (S > STOP) {
         constexpr int RLOG = S >= 4 ? 4 : S;
         if constexpr (TWO) {
             constexpr int half = THREADS / 2;
@@ -266,7 +266,7 @@ __device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twidd
             dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x);
         }
         __syncthreads();
-        dif_from<TWO, PR, LOGN, S - RLOG>(A0, A1, tw);
+        dif_from<TWO, PR, LOGN, S - RLOG, STOP>(A0, A1, tw);
     }
 }
 
@@ -287,6 +287,94 @@ __device__ __forceinline__ void dit_from(uint32_t *A0, uint32_t *A1, const Twidd
         __syncthreads();
         dit_from<TWO, PR, LOGN, LH0 + RLOG>(A0, A1, tw);
     }
+}
+
+// Radix of the last forward pass, which is also the first inverse pass: both
+// act on groups of R = 2^MID_RLOG consecutive elements with one twiddle set.
+template <int LOGN>
+constexpr int mid_rlog() {
+    return (LOGN & 3) ? (LOGN & 3) : 4;
+}
+
+// The last forward pass, the pointwise product and the first inverse pass in
+// one sweep over those groups (the three would otherwise each read and write
+// the whole transform in shared memory).  OP 0: square; OP 1: Montgomery
+// product with C (L2-coherent loads when CG: written in the same launch).
+template <int PR, int LOGN, int OP, bool CG, int STRIDE>
+__device__ __forceinline__ void mid_pass_t(uint32_t *__restrict__ A, const Twiddles &tw,
+                                           const uint32_t *__restrict__ C, int g0, const CrtConsts &cc) {
+    constexpr int RLOG = mid_rlog<LOGN>(), R = 1 << RLOG;
+    constexpr int GROUPS = (1 << LOGN) >> RLOG;
+    constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
+    uint32_t ta[R - 1], tsa[R - 1], tb[R - 1], tsb[R - 1];
+    if constexpr (RLOG == 4) {
+        load_wide<0, PR>(RLOG - 1, 0, ta, tsa);
+        load_wide<1, PR>(0, 0, tb, tsb);
+    } else {
+        load_tw<RLOG, false>(tw.w[PR], tw.wsh[PR], 0, 1, RLOG - 1, ta, tsa);
+        load_tw<RLOG, true>(tw.wi[PR], tw.wish[PR], 0, 1, 0, tb, tsb);
+    }
+#pragma unroll 1
+    for (int gg = g0; gg < GROUPS; gg += STRIDE) {
+        const int base = gg * R, pb = pad(base);  // R | 32: the group shares one pad offset
+        uint32_t v[R];
+#pragma unroll
+        for (int e = 0; e < R; e++) v[e] = A[pb + e];
+#pragma unroll
+        for (int s = 0, t0 = 0; s < RLOG; t0 += R >> (s + 1), s++) {  // forward, sub = 1
+            const int half = R >> (s + 1);
+#pragma unroll
+            for (int e = 0; e < R; e++) {
+                if (e & half) continue;
+                const int t = t0 + (e & (half - 1));
+                const uint32_t x = v[e], y = v[e + half];
+                v[e] = red2(x + y, p2);
+                v[e + half] = shoup(x - y + p2, ta[t], tsa[t], p);
+            }
+        }
+        if constexpr (OP == 0) {
+#pragma unroll
+            for (int e = 0; e < R; e++) v[e] = mont(v[e], v[e], p, cc.pinv[PR]);
+        } else {
+#pragma unroll
+            for (int e = 0; e < R; e++) v[e] = mont(v[e], CG ? __ldcg(C + base + e) : __ldg(C + base + e), p, cc.pinv[PR]);
+        }
+#pragma unroll
+        for (int s = 0, t0 = 0; s < RLOG; t0 += 1 << s, s++) {  // inverse, h0 = 1
+            const int half = 1 << s;
+#pragma unroll
+            for (int e = 0; e < R; e++) {
+                if (e & half) continue;
+                const int t = t0 + (e & (half - 1));
+                const uint32_t x = v[e];
+                const uint32_t u = shoup(v[e + half], tb[t], tsb[t], p);
+                v[e] = red2(x + u, p2);
+                v[e + half] = red2(x - u + p2, p2);
+            }
+        }
+#pragma unroll
+        for (int e = 0; e < R; e++) A[pb + e] = v[e];
+    }
+}
+
+// Forward transform, pointwise product and inverse transform of length
+// 2^LOGN: all forward passes but the last, the fused middle sweep, all
+// inverse passes but the first.  C0/C1: the stored spectra of the two primes
+// (OP 1).
+template <bool TWO, int PR, int LOGN, int OP, bool CG>
+__device__ __forceinline__ void product_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw, const uint32_t *C0,
+                                             const uint32_t *C1, const CrtConsts &cc) {
+    constexpr int M = mid_rlog<LOGN>();
+    dif_from<TWO, PR, LOGN, LOGN, M>(A0, A1, tw);
+    if constexpr (TWO) {
+        constexpr int half = THREADS / 2;
+        if ((int)threadIdx.x < half) mid_pass_t<0, LOGN, OP, CG, half>(A0, tw, C0, threadIdx.x, cc);
+        else mid_pass_t<1, LOGN, OP, CG, half>(A1, tw, C1, threadIdx.x - half, cc);
+    } else {
+        mid_pass_t<PR, LOGN, OP, CG, THREADS>(A0, tw, C0, threadIdx.x, cc);
+    }
+    __syncthreads();
+    dit_from<TWO, PR, LOGN, M>(A0, A1, tw);
 }
 
 #define PFB_LOGN_CASES(F) \
@@ -511,19 +599,8 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
             A1[pad(i)] = v;
         }
         __syncthreads();
-        dif_from<true, 0, LOGL, LOGL>(A0, A1, tw);
-        if (MUL && gy) {
-            pointwise2<true>(A0, A1, gy, gy + L, L, cc);
-        } else {
-            for (int i = tid; i < L; i += T) {
-                const int q = pad(i);
-                const uint32_t u = A0[q], v = A1[q];
-                A0[q] = mont(u, u, P1, cc.pinv[0]);
-                A1[q] = mont(v, v, P2, cc.pinv[1]);
-            }
-            __syncthreads();
-        }
-        dit_from<true, 0, LOGL, 0>(A0, A1, tw);
+        if (MUL && gy) product_from<true, 0, LOGL, 1, true>(A0, A1, tw, gy, gy + L, cc);
+        else product_from<true, 0, LOGL, 0, false>(A0, A1, tw, nullptr, nullptr, cc);
         // T = x^2 (or x y) as L limbs, in place over A0
         carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
         // S1 = T_lo + T_hi  -> X, carry cS
@@ -544,16 +621,12 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
         __syncthreads();
     }
     // m = T_lo * N' mod R
-    dif_from<true, 0, LOGL, LOGL>(A0, A1, tw);
-    pointwise2(A0, A1, cd.nph, cd.nph + L, L, cc);
-    dit_from<true, 0, LOGL, 0>(A0, A1, tw);
+    product_from<true, 0, LOGL, 1, false>(A0, A1, tw, cd.nph, cd.nph + L, cc);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
     for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1): cyclic product of length H
-    dif_from<true, 0, LOGL - 1, LOGL - 1>(A0, A1, tw);
-    pointwise2(A0, A1, cd.nh, cd.nh + H, H, cc);
-    dit_from<true, 0, LOGL - 1, 0>(A0, A1, tw);
+    product_from<true, 0, LOGL - 1, 1, false>(A0, A1, tw, cd.nh, cd.nh + H, cc);
     const unsigned long long cW =
         carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl - 1, cc); }, A0, cs);
     // U = S1 + W (mod R - 1); S1 = X (square = false: S1 = x itself)
@@ -615,30 +688,12 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     };
     if (square || (MUL && gy)) {
         load_x(X, false);
-        dif_from<false, 0, LOGL, LOGL>(A, nullptr, tw);
-        if (MUL && gy) {
-            pointwise1<0, true>(A, gy, L, cc);
-        } else {
-            for (int i = tid; i < L; i += T) {
-                const uint32_t u = A[pad(i)];
-                A[pad(i)] = mont(u, u, P1, cc.pinv[0]);
-            }
-            __syncthreads();
-        }
-        dit_from<false, 0, LOGL, 0>(A, nullptr, tw);
+        if (MUL && gy) product_from<false, 0, LOGL, 1, true>(A, nullptr, tw, gy, nullptr, cc);
+        else product_from<false, 0, LOGL, 0, false>(A, nullptr, tw, nullptr, nullptr, cc);
         spill_L();
         load_x(X, false);
-        dif_from<false, 1, LOGL, LOGL>(A, nullptr, tw);
-        if (MUL && gy) {
-            pointwise1<1, true>(A, gy + L, L, cc);
-        } else {
-            for (int i = tid; i < L; i += T) {
-                const uint32_t u = A[pad(i)];
-                A[pad(i)] = mont(u, u, P2, cc.pinv[1]);
-            }
-            __syncthreads();
-        }
-        dit_from<false, 1, LOGL, 0>(A, nullptr, tw);
+        if (MUL && gy) product_from<false, 1, LOGL, 1, true>(A, nullptr, tw, gy + L, nullptr, cc);
+        else product_from<false, 1, LOGL, 0, false>(A, nullptr, tw, nullptr, nullptr, cc);
         carry_pass<true>(
             L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<L>(i)), A[pad(i)], logl, cc); }, A, cs);
         cS = carry_pass<true>(H, 0ull,
@@ -651,28 +706,20 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
         load_x(X, false);
     }
     // m = T_lo * N' mod R
-    dif_from<false, 0, LOGL, LOGL>(A, nullptr, tw);
-    pointwise1<0>(A, cd.nph, L, cc);
-    dit_from<false, 0, LOGL, 0>(A, nullptr, tw);
+    product_from<false, 0, LOGL, 1, false>(A, nullptr, tw, cd.nph, nullptr, cc);
     spill_H();
     load_x(sp.t, true);
-    dif_from<false, 1, LOGL, LOGL>(A, nullptr, tw);
-    pointwise1<1>(A, cd.nph + L, L, cc);
-    dit_from<false, 1, LOGL, 0>(A, nullptr, tw);
+    product_from<false, 1, LOGL, 1, false>(A, nullptr, tw, cd.nph + L, nullptr, cc);
     carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl, cc); }, A, cs);
     for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
     __syncthreads();
     // W = m * N mod (R - 1)
-    dif_from<false, 0, LOGL - 1, LOGL - 1>(A, nullptr, tw);
-    pointwise1<0>(A, cd.nh, H, cc);
-    dit_from<false, 0, LOGL - 1, 0>(A, nullptr, tw);
+    product_from<false, 0, LOGL - 1, 1, false>(A, nullptr, tw, cd.nh, nullptr, cc);
     spill_H();
     for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
     __syncthreads();
-    dif_from<false, 1, LOGL - 1, LOGL - 1>(A, nullptr, tw);
-    pointwise1<1>(A, cd.nh + H, H, cc);
-    dit_from<false, 1, LOGL - 1, 0>(A, nullptr, tw);
+    product_from<false, 1, LOGL - 1, 1, false>(A, nullptr, tw, cd.nh + H, nullptr, cc);
     const unsigned long long cW = carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl - 1, cc); }, A, cs);
     unsigned long long c = carry_pass<true>(
