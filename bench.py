@@ -186,6 +186,37 @@ def cpu_sieve_baseline(procs=None, frac=0.05):
                       "one process per core, scaled by prime count" % int(frac * 100)}
 
 
+# small cases of the squaring kernel for ncu captures: N and rev(N) of four
+# (k, j) at one (a, b, c), 8 candidates (one CTA each), one launch of 64 squarings
+MR_CASES = {
+    "50k": ((50000, 30000, 100), None),  # the first four survivors of (50000, 30000, 100)
+    "100k": ((100000, 60000, 100), [(1, 99), (2, 84), (4, 60), (5, 84)]),
+}
+
+
+def mr_case(name):
+    """Run one small case of the persistent squaring kernel and print its time."""
+    import torch
+    import pfb200
+    abc, pairs = MR_CASES[name]
+    if pairs is None:
+        g = json.load(open(os.path.join(ROOT, "tests", "golden", "sieve_50000_30000_100.json")))
+        pairs = [tuple(x) for x in g["survivors_99"][:4]]
+    cands = [pfb200.build_candidate(*abc, k, j, rev) for (k, j) in pairs for rev in (False, True)]
+    eng = pfb200.MillerRabin(0)
+    batch = pfb200.MRBatch(eng, cands, 2)
+    stream = torch.cuda.Stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.advance(64, stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    print(json.dumps({"case": name, "candidates": len(cands), "squarings": 64,
+                      "ms": e0.elapsed_time(e1), "steps_done": pfb200.batch_steps_done(batch)}))
+    batch.close()
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -201,7 +232,12 @@ def main():
     ap.add_argument("--serve-secs", type=float, default=0.0,
                     help="also run the serving loop (Poisson arrivals of 50k-100k-digit requests) this long")
     ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
+    ap.add_argument("--mr-case", choices=sorted(MR_CASES),
+                    help="only run a small case of the squaring kernel (8 candidates, 64 squarings; for ncu)")
     args = ap.parse_args()
+    if args.mr_case:
+        mr_case(args.mr_case)
+        return
 
     rank, world, local = replicas.rank_world()
     abc1 = (50000, 30000, 100)
