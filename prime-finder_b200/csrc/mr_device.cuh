@@ -122,20 +122,22 @@ __device__ __forceinline__ void load_tw(const uint32_t *__restrict__ W, const ui
 // element offsets inside a group.  When every group of a thread has the same
 // j0 (all passes but the widest) its twiddles are loaded once per pass.
 
-template <int PR, int RLOG, int SUB>
+// ZHI: the group's upper half (e >= R/2) is known to be zero and is not read;
+// the lower half holds limbs (< 2p), so the first stage is x, x w.
+template <int PR, int RLOG, int SUB, bool ZHI = false>
 __device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, const uint32_t *tw,
                                             const uint32_t *tws) {
-    constexpr int R = 1 << RLOG;
+    constexpr int R = 1 << RLOG, NL = ZHI ? R / 2 : R;
     constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
     uint32_t v[R];
     if constexpr (SUB % 32 == 0) {
         constexpr int PS = SUB + SUB / 32;  // pad(base + e SUB) = pad(base) + e PS
         const int pb = pad(base);
 #pragma unroll
-        for (int e = 0; e < R; e++) v[e] = A[pb + e * PS];
+        for (int e = 0; e < NL; e++) v[e] = A[pb + e * PS];
     } else {
 #pragma unroll
-        for (int e = 0; e < R; e++) v[e] = A[pad(base + e * SUB)];
+        for (int e = 0; e < NL; e++) v[e] = A[pad(base + e * SUB)];
     }
 #pragma unroll
     for (int s = 0, t0 = 0; s < RLOG; t0 += R >> (s + 1), s++) {
@@ -144,6 +146,10 @@ __device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, 
         for (int e = 0; e < R; e++) {
             if (e & half) continue;
             const int t = t0 + (e & (half - 1));
+            if (ZHI && s == 0) {
+                v[e + half] = shoup(v[e], tw[t], tws[t], p);
+                continue;
+            }
             const uint32_t x = v[e], y = v[e + half];
             v[e] = red2(x + y, p2);
             v[e + half] = shoup(x - y + p2, tw[t], tws[t], p);
@@ -199,7 +205,7 @@ __device__ __forceinline__ void dit_group_t(uint32_t *__restrict__ A, int base, 
     }
 }
 
-template <int PR, int RLOG, int LOGN, int LH0, int STRIDE>
+template <int PR, int RLOG, int LOGN, int LH0, int STRIDE, bool ZHI = false>
 __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint32_t *__restrict__ W,
                                            const uint32_t *__restrict__ Wsh, int g0) {
     constexpr int R = 1 << RLOG, H0 = 1 << LH0;
@@ -212,7 +218,7 @@ __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint3
 #pragma unroll 1
         for (int gg = g0; gg < GROUPS; gg += STRIDE) {
             const int block = gg / SUB, j0 = gg % SUB;
-            dif_group_t<PR, RLOG, SUB>(A, block * 2 * H0 + j0, ta, tsa);
+            dif_group_t<PR, RLOG, SUB, ZHI>(A, block * 2 * H0 + j0, ta, tsa);
         }
     } else {
 #pragma unroll 1
@@ -220,7 +226,7 @@ __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint3
             const int block = gg / SUB, j0 = gg % SUB;
             if constexpr (RLOG == 4) load_wide<0, PR>(LH0, j0, ta, tsa);
             else load_tw<RLOG, false>(W, Wsh, j0, SUB, LH0, ta, tsa);
-            dif_group_t<PR, RLOG, SUB>(A, block * 2 * H0 + j0, ta, tsa);
+            dif_group_t<PR, RLOG, SUB, ZHI>(A, block * 2 * H0 + j0, ta, tsa);
         }
     }
 }
@@ -251,19 +257,22 @@ __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint3
 }
 
 // Forward passes from S remaining stages down (h0 = 2^(S-1)); two primes
-// split the CTA (TWO) or one prime uses all of it.
-template <bool TWO, int PR, int LOGN, int S, int STOP = 0>
+// split the CTA (TWO) or one prime uses all of it.  ZHI (first pass only,
+// S = LOGN): the input's upper half is zero and is neither read nor stored
+// beforehand (a zero-padded operand of a full-length product).
+template <bool TWO, int PR, int LOGN, int S, int STOP = 0, bool ZHI = false>
 __device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
+    static_assert(!ZHI || (S == LOGN && S >= 4), "ZHI: first radix-16 pass of the transform");
     if constexpr (S > STOP) {
         constexpr int RLOG = S >= 4 ? 4 : S;
         if constexpr (TWO) {
             constexpr int half = THREADS / 2;
             if ((int)threadIdx.x < half)
-                dif_pass_t<0, RLOG, LOGN, S - 1, half>(A0, tw.w[0], tw.wsh[0], threadIdx.x);
+                dif_pass_t<0, RLOG, LOGN, S - 1, half, ZHI>(A0, tw.w[0], tw.wsh[0], threadIdx.x);
             else
-                dif_pass_t<1, RLOG, LOGN, S - 1, half>(A1, tw.w[1], tw.wsh[1], threadIdx.x - half);
+                dif_pass_t<1, RLOG, LOGN, S - 1, half, ZHI>(A1, tw.w[1], tw.wsh[1], threadIdx.x - half);
         } else {
-            dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x);
+            dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS, ZHI>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x);
         }
         __syncthreads();
         dif_from<TWO, PR, LOGN, S - RLOG, STOP>(A0, A1, tw);
@@ -360,12 +369,12 @@ __device__ __forceinline__ void mid_pass_t(uint32_t *__restrict__ A, const Twidd
 // Forward transform, pointwise product and inverse transform of length
 // 2^LOGN: all forward passes but the last, the fused middle sweep, all
 // inverse passes but the first.  C0/C1: the stored spectra of the two primes
-// (OP 1).
-template <bool TWO, int PR, int LOGN, int OP, bool CG>
+// (OP 1).  ZHI: the operand's upper half is zero and was never stored.
+template <bool TWO, int PR, int LOGN, int OP, bool CG, bool ZHI = false>
 __device__ __forceinline__ void product_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw, const uint32_t *C0,
                                              const uint32_t *C1, const CrtConsts &cc) {
     constexpr int M = mid_rlog<LOGN>();
-    dif_from<TWO, PR, LOGN, LOGN, M>(A0, A1, tw);
+    dif_from<TWO, PR, LOGN, LOGN, M, ZHI>(A0, A1, tw);
     if constexpr (TWO) {
         constexpr int half = THREADS / 2;
         if ((int)threadIdx.x < half) mid_pass_t<0, LOGN, OP, CG, half>(A0, tw, C0, threadIdx.x, cc);
@@ -592,36 +601,28 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
     const int tid = threadIdx.x, T = blockDim.x;
     unsigned long long cS = 0;  // carry of T_lo + T_hi
 
+    // the operands of the two length-L products are H limbs, zero above:
+    // only the lower halves are stored (the first forward pass takes the
+    // upper halves as zero)
+    for (int i = tid; i < H; i += T) {
+        const uint32_t v = X[pad(i)];
+        A0[pad(i)] = v;
+        A1[pad(i)] = v;
+    }
+    __syncthreads();
     if (square || (MUL && gy)) {
-        for (int i = tid; i < L; i += T) {
-            const uint32_t v = i < H ? X[pad(i)] : 0u;
-            A0[pad(i)] = v;
-            A1[pad(i)] = v;
-        }
-        __syncthreads();
-        if (MUL && gy) product_from<true, 0, LOGL, 1, true>(A0, A1, tw, gy, gy + L, cc);
-        else product_from<true, 0, LOGL, 0, false>(A0, A1, tw, nullptr, nullptr, cc);
+        if (MUL && gy) product_from<true, 0, LOGL, 1, true, true>(A0, A1, tw, gy, gy + L, cc);
+        else product_from<true, 0, LOGL, 0, false, true>(A0, A1, tw, nullptr, nullptr, cc);
         // T = x^2 (or x y) as L limbs, in place over A0
         carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
         // S1 = T_lo + T_hi  -> X, carry cS
         cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A0[pad(i)] + A0[pad(i + H)]; }, X, cs);
-        for (int i = tid; i < L; i += T) {
-            const int q = pad(i);
-            if (i < H) A1[q] = A0[q];
-            else A0[q] = A1[q] = 0u;
-        }
-        __syncthreads();
-    } else {
-        for (int i = tid; i < L; i += T) {
-            const uint32_t v = i < H ? X[pad(i)] : 0u;
-            A0[pad(i)] = v;
-            A1[pad(i)] = v;
-        }
+        for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
         __syncthreads();
     }
     // m = T_lo * N' mod R
-    product_from<true, 0, LOGL, 1, false>(A0, A1, tw, cd.nph, cd.nph + L, cc);
+    product_from<true, 0, LOGL, 1, false, true>(A0, A1, tw, cd.nph, cd.nph + L, cc);
     carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
     for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
     __syncthreads();
@@ -671,8 +672,10 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     const int tid = threadIdx.x;
     constexpr int T = THREADS;
     unsigned long long cS = 0;
+    // lower half of a length-L product's operand (the upper half is zero and
+    // is taken as such by the first forward pass)
     auto load_x = [&](const uint32_t *src, bool from_global) {
-        for (int i = tid; i < L; i += T) A[pad(i)] = i < H ? (from_global ? ldg_spill(src + i) : src[pad(i)]) : 0u;
+        for (int i = tid; i < H; i += T) A[pad(i)] = from_global ? ldg_spill(src + i) : src[pad(i)];
         __syncthreads();
     };
     // coalesced writes: slot j holds position (j mod T) w + j / T
@@ -688,28 +691,27 @@ __device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint3
     };
     if (square || (MUL && gy)) {
         load_x(X, false);
-        if (MUL && gy) product_from<false, 0, LOGL, 1, true>(A, nullptr, tw, gy, nullptr, cc);
-        else product_from<false, 0, LOGL, 0, false>(A, nullptr, tw, nullptr, nullptr, cc);
+        if (MUL && gy) product_from<false, 0, LOGL, 1, true, true>(A, nullptr, tw, gy, nullptr, cc);
+        else product_from<false, 0, LOGL, 0, false, true>(A, nullptr, tw, nullptr, nullptr, cc);
         spill_L();
         load_x(X, false);
-        if (MUL && gy) product_from<false, 1, LOGL, 1, true>(A, nullptr, tw, gy + L, nullptr, cc);
-        else product_from<false, 1, LOGL, 0, false>(A, nullptr, tw, nullptr, nullptr, cc);
+        if (MUL && gy) product_from<false, 1, LOGL, 1, true, true>(A, nullptr, tw, gy + L, nullptr, cc);
+        else product_from<false, 1, LOGL, 0, false, true>(A, nullptr, tw, nullptr, nullptr, cc);
         carry_pass<true>(
             L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<L>(i)), A[pad(i)], logl, cc); }, A, cs);
         cS = carry_pass<true>(H, 0ull,
                                [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
         for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
-        for (int i = H + tid; i < L; i += T) A[pad(i)] = 0u;
         __syncthreads();
     } else {
         for (int i = tid; i < H; i += T) sp.t[i] = X[pad(i)];
         load_x(X, false);
     }
     // m = T_lo * N' mod R
-    product_from<false, 0, LOGL, 1, false>(A, nullptr, tw, cd.nph, nullptr, cc);
+    product_from<false, 0, LOGL, 1, false, true>(A, nullptr, tw, cd.nph, nullptr, cc);
     spill_H();
     load_x(sp.t, true);
-    product_from<false, 1, LOGL, 1, false>(A, nullptr, tw, cd.nph + L, nullptr, cc);
+    product_from<false, 1, LOGL, 1, false, true>(A, nullptr, tw, cd.nph + L, nullptr, cc);
     carry_pass<true>(
         H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl, cc); }, A, cs);
     for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
