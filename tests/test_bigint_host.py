@@ -1,0 +1,133 @@
+"""The engine's host multi-precision helpers (prime-finder_b200/csrc/bigint_host.h)
+against Python integers, on the CPU.
+
+These compute the per-modulus set-up the reference does with GMP
+(barrett.cu:58-107, montgomery.cu:30-45): N' = -N^-1 mod 2^bits by Hensel
+lifting, 2^e mod N by Knuth's long division, the candidate's powers of ten,
+and the limb conversions between the reference's 16-bit format and the
+engine's 22-bit limbs.  A small driver (tests/cpp/bigint_host_check.cpp)
+is compiled against the header and fed random and edge-case operands.
+"""
+import math
+import os
+import random
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.set_int_max_str_digits(0)
+
+
+@pytest.fixture(scope="module")
+def run(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("bigint") / "bigint_host_check")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "prime-finder_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "cpp", "bigint_host_check.cpp"), "-o", exe], check=True)
+
+    def go(lines):
+        out = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True,
+                             check=True).stdout.split("\n")
+        return out[:len(lines)]
+    return go
+
+
+def h(x):
+    return format(x, "x")
+
+
+def _candidate(a, b, c, k, j):
+    return 10 ** a - k * 10 ** b - j * 10 ** c - 1
+
+
+def test_divmod(run):
+    rng = random.Random(1)
+    cases = []
+    for _ in range(150):
+        nb = rng.choice([32, 64, 65, 200, 1000, 5000])
+        v = rng.getrandbits(nb) | 1
+        u = rng.getrandbits(nb + rng.choice([0, 1, 31, 32, 33, 300, 3000]))
+        cases.append((u, v))
+    cases += [(0, 5), (7, 7), (6, 7), (14, 7), ((1 << 640) - 1, (1 << 320) - 1), (1 << 500, (1 << 64) + 1)]
+    # a quotient digit estimate that is one too large (the add-back step of algorithm D)
+    cases.append(((0x7FFFFFFF << 96) | (0x80000000 << 64), (0x80000000 << 64) | 1))
+    cases.append(((0x7FFF800000000000 << 128), (0x800000000000 << 64) + 1))
+    N = _candidate(3000, 1700, 100, 7, 19)
+    cases.append((N * N + 12345, N))
+    out = run(["divmod %s %s" % (h(u), h(v)) for u, v in cases])
+    for (u, v), line in zip(cases, out):
+        q, r = (int(t, 16) for t in line.split())
+        assert (q, r) == divmod(u, v), (u, v)
+
+
+def test_pow2_mod_and_neg_inv_at_transform_sizes(run):
+    """The set-up of a 50 000-digit candidate at L = 2^14 (R = 2^(22 * 8192))
+    and of smaller ones at other lengths."""
+    rng = random.Random(2)
+    Ns = [_candidate(50000, 30000, 100, 1, 99), _candidate(2000, 1000, 100, 5, 84)]
+    Ns += [rng.getrandbits(b) | 1 | (1 << (b - 1)) for b in (3, 63, 64, 65, 700, 4000)]
+    lines, want = [], []
+    for N in Ns:
+        rbits = 22 * 8192 if N.bit_length() > 100000 else 22 * (1 << max(1, (N.bit_length() // 22 + 2).bit_length()))
+        lines.append("pow2_mod %d %s" % (rbits, h(N)))
+        want.append(pow(2, rbits, N))
+        lines.append("neg_inv %s %d" % (h(N), rbits))
+        want.append((-pow(N, -1, 1 << rbits)) % (1 << rbits))
+    out = run(lines)
+    assert [int(x, 16) for x in out] == want
+
+
+def test_arithmetic_and_shifts(run):
+    rng = random.Random(3)
+    lines, want = [], []
+    for _ in range(60):
+        a = rng.getrandbits(rng.choice([1, 64, 65, 128, 900]))
+        b = rng.getrandbits(rng.choice([1, 64, 65, 128, 900]))
+        s = rng.choice([0, 1, 63, 64, 65, 200])
+        lines += ["mul %s %s" % (h(a), h(b)), "sub %s %s" % (h(max(a, b)), h(min(a, b))),
+                  "shl %s %d" % (h(a), s), "shr %s %d" % (h(a), s)]
+        want += [a * b, max(a, b) - min(a, b), a << s, a >> s]
+    for m in (3, 7, 65521, 4294967291):
+        a = rng.getrandbits(3000)
+        lines.append("mod_small %s %d" % (h(a), m))
+        want.append(a % m)
+    out = run(lines)
+    got = [int(x, 16) if not l.startswith("mod_small") else int(x) for l, x in zip(lines, out)]
+    assert got == want
+
+
+def test_isqrt(run):
+    rng = random.Random(4)
+    vals = [1, 2, 3, 4, 15, 16, 17, (1 << 128) - 1, 1 << 128]
+    for b in (40, 200, 2000):
+        r = rng.getrandbits(b)
+        vals += [r * r - 1, r * r, r * r + 1, r * r + 2 * r]
+    out = run(["isqrt %s" % h(v) for v in vals])
+    assert [int(x, 16) for x in out] == [math.isqrt(v) for v in vals]
+
+
+def test_pow10(run):
+    es = [0, 1, 2, 19, 20, 27, 28, 100, 1001, 50000]
+    out = run(["pow10 %d" % e for e in es])
+    assert [int(x, 16) for x in out] == [10 ** e for e in es]
+
+
+def test_limb_round_trips(run):
+    rng = random.Random(5)
+    lines, want = [], []
+    for bits in (16, 22, 32):
+        for n in (1, 2, 3, 7, 8192):
+            a = rng.getrandbits(bits * n)
+            lines.append("limbs %s %d %d" % (h(a), bits, n))
+            want.append(a)
+            # truncation: only the low n limbs are kept
+            big = a | (rng.getrandbits(50) << (bits * n))
+            lines.append("limbs %s %d %d" % (h(big), bits, n))
+            want.append(a)
+    for n in (1, 4, 5, 10386):
+        a = rng.getrandbits(16 * n)
+        lines.append("u16 %s %d" % (h(a), n))
+        want.append(a)
+    out = run(lines)
+    assert [int(x, 16) for x in out] == want
