@@ -8,12 +8,15 @@
 //   mul A B / sub A B / shl A s / shr A s / isqrt A / pow10 e / mod_small A m
 //   limbs A bits n    -> from_limbs(to_limbs(A)) (round trip through n limbs)
 //   u16 A n           -> from_u16(to_u16(A))     (round trip through n limbs)
+//   build a b c k j r -> N (r = 0) or rev(N) (r = 1) of phase2_host.h, "-" if
+//                        the reference formula gives no positive number
 #include <cstdio>
 #include <iostream>
 #include <sstream>
 #include <string>
 
 #include "bigint_host.h"
+#include "phase2_host.h"
 
 using namespace pfb::big;
 
@@ -83,6 +86,13 @@ int main() {
             std::vector<uint16_t> l(n);
             to_u16(from_hex(x), l.data(), n);
             std::cout << to_hex(from_u16(l.data(), n)) << "\n";
+        } else if (op == "build") {
+            long long v[6] = {0, 0, 0, 0, 0, 0};
+            std::istringstream all(line.substr(op.size()));
+            for (auto &t : v) all >> t;
+            const Words w = v[5] ? pfb::phase2::build_rev(v[0], v[1], v[2], (int)v[3], (int)v[4])
+                                 : pfb::phase2::build_n(v[0], v[1], v[2], (int)v[3], (int)v[4]);
+            std::cout << (w.empty() ? std::string("-") : to_hex(w)) << "\n";
         } else {
             std::cout << "?\n";
         }

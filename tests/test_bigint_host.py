@@ -4,8 +4,11 @@ against Python integers, on the CPU.
 These compute the per-modulus set-up the reference does with GMP
 (barrett.cu:58-107, montgomery.cu:30-45): N' = -N^-1 mod 2^bits by Hensel
 lifting, 2^e mod N by Knuth's long division, the candidate's powers of ten,
-and the limb conversions between the reference's 16-bit format and the
-engine's 22-bit limbs.  A small driver (tests/cpp/bigint_host_check.cpp)
+the limb conversions between the reference's 16-bit format and the
+engine's 22-bit limbs, and the candidates N and rev(N) that miller_rabin_test
+and the sieve -> test pipeline build (phase2_host.h, miller_rabin.c:32-74),
+against the oracle's restatement of the reference's build_N/build_revN.  A
+small driver (tests/cpp/bigint_host_check.cpp)
 is compiled against the header and fed random and edge-case operands.
 """
 import math
@@ -24,7 +27,7 @@ sys.set_int_max_str_digits(0)
 def run(tmp_path_factory):
     exe = str(tmp_path_factory.mktemp("bigint") / "bigint_host_check")
     subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "prime-finder_b200", "csrc"),
-                    os.path.join(ROOT, "tests", "cpp", "bigint_host_check.cpp"), "-o", exe], check=True)
+                    "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "bigint_host_check.cpp"), "-o", exe], check=True)
 
     def go(lines):
         out = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True,
@@ -131,3 +134,32 @@ def test_limb_round_trips(run):
         want.append(a)
     out = run(lines)
     assert [int(x, 16) for x in out] == want
+
+
+def test_candidates_equal_the_reference_formula(run):
+    """N = 10^a - k 10^b - j 10^c - 1 and rev(N) = 10^a - rev(k) 10^(a-b-lk)
+    - rev(j) 10^(a-c-lj) - 1, including the tuples where rev(N) is not the
+    literal digit reversal (overlapping blocks, b + lk >= a) and the ones with
+    a negative exponent or a non-positive result, which both reject."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    rng = random.Random(6)
+    tuples = [(50000, 30000, 100, 1, 99), (100000, 60000, 100, 5, 84), (4, 2, 1, 3, 7), (3, 2, 1, 9, 9),
+              (5, 3, 1, 99, 9), (6, 4, 0, 1000, 1), (2, 1, 0, 1, 1), (1, 0, 0, 5, 4), (12, 5, 2, 9999, 10)]
+    for _ in range(80):
+        a = rng.randint(2, 400)
+        b = rng.randint(0, a)
+        c = rng.randint(0, b)
+        tuples.append((a, b, c, rng.randint(1, 9999), rng.randint(1, 9999)))
+    lines, want = [], []
+    for a, b, c, k, j in tuples:
+        for rev in (0, 1):
+            lines.append("build %d %d %d %d %d %d" % (a, b, c, k, j, rev))
+            try:
+                want.append(oracle.build_candidate(a, b, c, k, j, bool(rev)))
+            except ValueError:
+                want.append(None)
+    out = run(lines)
+    got = [None if x == "-" else int(x, 16) for x in out]
+    assert got == want
+    assert sum(w is None for w in want) > 5 and sum(w is not None for w in want) > 100
