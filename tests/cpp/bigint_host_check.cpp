@@ -10,12 +10,14 @@
 //   u16 A n           -> from_u16(to_u16(A))     (round trip through n limbs)
 //   build a b c k j r -> N (r = 0) or rev(N) (r = 1) of phase2_host.h, "-" if
 //                        the reference formula gives no positive number
+//   selfridge N       -> "1 D" (Selfridge's D), "0" (composite found), "-1"
 #include <cstdio>
 #include <iostream>
 #include <sstream>
 #include <string>
 
 #include "bigint_host.h"
+#include "lucas_host.h"
 #include "phase2_host.h"
 
 using namespace pfb::big;
@@ -93,6 +95,11 @@ int main() {
             const Words w = v[5] ? pfb::phase2::build_rev(v[0], v[1], v[2], (int)v[3], (int)v[4])
                                  : pfb::phase2::build_n(v[0], v[1], v[2], (int)v[3], (int)v[4]);
             std::cout << (w.empty() ? std::string("-") : to_hex(w)) << "\n";
+        } else if (op == "selfridge") {
+            long D = 0;
+            const int r = pfb::mr::selfridge(from_hex(x), D);
+            if (r == 1) std::cout << "1 " << D << "\n";
+            else std::cout << r << "\n";
         } else {
             std::cout << "?\n";
         }

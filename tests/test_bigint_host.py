@@ -7,8 +7,9 @@ lifting, 2^e mod N by Knuth's long division, the candidate's powers of ten,
 the limb conversions between the reference's 16-bit format and the
 engine's 22-bit limbs, and the candidates N and rev(N) that miller_rabin_test
 and the sieve -> test pipeline build (phase2_host.h, miller_rabin.c:32-74),
-against the oracle's restatement of the reference's build_N/build_revN.  A
-small driver (tests/cpp/bigint_host_check.cpp)
+against the oracle's restatement of the reference's build_N/build_revN, and
+Selfridge's parameters for the strong Lucas test (lucas_host.h) against the
+oracle's restatement (oracle/lucas.py).  A small driver (tests/cpp/bigint_host_check.cpp)
 is compiled against the header and fed random and edge-case operands.
 """
 import math
@@ -163,3 +164,20 @@ def test_candidates_equal_the_reference_formula(run):
     got = [None if x == "-" else int(x, 16) for x in out]
     assert got == want
     assert sum(w is None for w in want) > 5 and sum(w is not None for w in want) > 100
+
+
+def test_selfridge_parameters(run):
+    """D of Selfridge's method A (or "composite": a proper factor |D|, or a
+    perfect square) for every odd n < 20 000 and for large numbers of each
+    kind, equal to the oracle's restatement."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import lucas
+    rng = random.Random(7)
+    ns = list(range(3, 20001, 2))
+    ns += [rng.getrandbits(b) | 1 for b in (33, 64, 65, 500, 3000) for _ in range(10)]
+    ns += [(rng.getrandbits(b) | 1) ** 2 for b in (20, 40, 300)]
+    ns += [p * (rng.getrandbits(200) | 1) for p in (5, 7, 11, 13, 17, 19, 23)]
+    out = run(["selfridge %s" % h(n) for n in ns])
+    for n, line in zip(ns, out):
+        want = lucas.selfridge_d(n)
+        assert line == ("0" if want is None else "1 %d" % want), n
