@@ -65,7 +65,12 @@ void pfb_sieve_destroy(pfb_sieve_t *s);
  * trial_div_kernel (trial_div.cu:82-159) and sieve_one_prime
  * (trial_div_cpu.c:32-102), for any K.  stream is a cudaStream_t (NULL = the
  * context's own stream).  With a device mask the call is asynchronous; with
- * PFB_SIEVE_MASK_HOST it copies in/out and synchronises.
+ * PFB_SIEVE_MASK_HOST it copies in/out and synchronises.  A call with a
+ * different K than the previous one first waits for `stream` (the context
+ * re-splits its prime list).  The context's working buffers are reused by
+ * every call: calls on one context must be issued on one stream (or from one
+ * thread with the stream synchronised between them); use one context per
+ * concurrent stream.
  */
 int pfb_sieve_run(pfb_sieve_t *s, const long long *abc, int n_abc, int K,
                   uint8_t *mask, unsigned flags, void *stream);
@@ -75,7 +80,8 @@ int pfb_sieve_run(pfb_sieve_t *s, const long long *abc, int n_abc, int K,
  * device mask block, writes the surviving (k,j) (bit = 0) in k-major order as
  * uint32 (k << 16 | j) to d_out (device, capacity cap) and their number to
  * *count (host).  Synchronises on the stream.  Returns PFB_E_CAPACITY, with
- * *count set, if cap is too small.
+ * *count set, if cap is too small.  Shares the context's working buffers
+ * with pfb_sieve_run (same stream rule).
  */
 int pfb_sieve_survivors(pfb_sieve_t *s, const uint8_t *d_mask, int K,
                         uint32_t *d_out, uint32_t cap, uint32_t *count, void *stream);

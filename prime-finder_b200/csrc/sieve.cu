@@ -833,7 +833,11 @@ extern "C" int pfb_sieve_run(pfb_sieve_t *s, const long long *abc, int n_abc, in
         PFB_CUDA(cudaMalloc(&s->d_abc, sizeof(long long) * 3 * n_abc));
         s->abc_cap = n_abc;
     }
-    // ensure_split runs on the context stream; order it before st.
+    // ensure_split runs on the context stream and synchronises it, which
+    // orders it before st.  A new K re-splits the prime list in place, so
+    // earlier work queued on another stream (still reading the lists) must
+    // finish first.
+    if (small_limit(K) != s->s_limit && st != s->stream) PFB_CUDA(cudaStreamSynchronize(st));
     int rc = ensure_split(s, K);
     if (rc) return rc;
     PFB_CUDA(cudaMemcpyAsync(s->d_abc, abc, sizeof(long long) * 3 * n_abc, cudaMemcpyHostToDevice, st));
