@@ -1086,9 +1086,19 @@ int run_jobs(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, int m
     rc = batch_advance(b, b->max_steps, e->stream);
     // The round-robin hands a locked candidate's quantum to another one, so a
     // few candidates may still need steps: continue until none is pending.
-    for (int pending = 1; !rc;) {
+    // Every round advances each unfinished candidate, so a round count of
+    // max_steps / 4096 + 64 is never reached unless the device stopped
+    // making progress.
+    const long long max_rounds = b->max_steps / 4096 + 64;
+    for (long long round = 0; !rc; round++) {
+        int pending = 0;
         rc = batch_pending(b, &pending, nullptr);
         if (rc || pending == 0) break;
+        if (round >= max_rounds) {
+            pfb::set_error("pfb_mr: %d candidates unfinished after %lld extra rounds", pending, round);
+            rc = PFB_E_STATE;
+            break;
+        }
         rc = batch_advance(b, 4096, e->stream);
     }
     if (!rc) rc = batch_results(b, verdict, residue, residue_stride);
