@@ -121,6 +121,10 @@ void pfb_mr_batch_destroy(pfb_mr_batch_t *b);
  * chunk_steps per launch of the persistent kernel (candidates of different
  * lengths share every launch), and retires finished ones.  Per-candidate
  * residue and exponent cursor live in device memory for the whole test.
+ * If a slot allocation fails below the budget (device memory held
+ * elsewhere), the server frees its pooled slot memory and retries; failing
+ * that, the request waits until resident candidates retire, or gets verdict
+ * -1 when none is resident.
  */
 typedef struct pfb_mr_server pfb_mr_server_t;
 

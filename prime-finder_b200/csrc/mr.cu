@@ -1475,9 +1475,46 @@ int srv_admit(pfb_mr_server *s, std::vector<int> &admitted) {
         SrvSlot &sl = s->slots[admitted.back()];
         if (!sl.mem) {
             const size_t need = slot_bytes(sl.logl);
-            if (cudaMalloc(&sl.mem, need) != cudaSuccess) {
+            cudaError_t ce = cudaMalloc(&sl.mem, need);
+            if (ce != cudaSuccess) {
+                // the device ran out below the budget (memory held elsewhere):
+                // give back the pooled blocks and try once more
                 cudaGetLastError();
-                return PFB_E_NOMEM;
+                std::lock_guard<std::mutex> lk(s->mu);
+                for (auto &kv : s->pool) {
+                    const size_t blk = slot_bytes(kv.first);
+                    for (uint8_t *m : kv.second) {
+                        cudaFree(m);
+                        s->bytes_owned -= std::min(s->bytes_owned, blk);
+                    }
+                    kv.second.clear();
+                }
+                sl.mem = nullptr;
+                ce = cudaMalloc(&sl.mem, need);
+            }
+            if (ce != cudaSuccess) {
+                // undo the admission: the request waits for resident candidates
+                // to retire, or fails if none is resident
+                cudaGetLastError();
+                sl.mem = nullptr;
+                admitted.pop_back();
+                std::lock_guard<std::mutex> lk(s->mu);
+                sl.busy = false;
+                s->bytes_in_use -= need;
+                if (s->resident == 0 && admitted.empty()) {
+                    pfb_mr_result_t res{};
+                    res.tag = sl.req.tag;
+                    res.verdict = -1;
+                    res.submit_s = sl.req.t_submit;
+                    res.admit_s = res.done_s = now_s(s);
+                    s->done.push_back(res);
+                    s->n_completed++;
+                    s->cv_done.notify_all();
+                } else {
+                    s->prepared.push_front(std::move(sl.req));
+                }
+                sl.req = SrvRequest();
+                break;
             }
             std::lock_guard<std::mutex> lk(s->mu);
             s->bytes_owned += need;
