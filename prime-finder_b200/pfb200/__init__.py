@@ -3,7 +3,8 @@
 The engine is the shared library ``prime-finder_b200/lib/libpfb200.so``
 built from ``prime-finder_b200/csrc`` (sm_100a CUDA + C ABI).  This module
 only marshals arguments; every computation runs in the library.  If the
-library is missing the import fails: there is no CPU fallback.
+library is missing, the first call into it raises ImportError: there is no
+CPU fallback.
 
 Device buffers may be given as integers (raw device pointers) or as any
 object with ``data_ptr()`` (e.g. a CUDA ``torch.Tensor``).
