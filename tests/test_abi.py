@@ -55,3 +55,16 @@ def test_every_declared_symbol_is_exported():
         except AttributeError:
             missing.append(name)
     assert not missing, missing
+
+
+def test_missing_library_raises_instead_of_falling_back(tmp_path):
+    """With the shared library absent, the binding's first call raises
+    ImportError (there is no CPU path to fall back to).  A fresh interpreter
+    with the package's library path pointed at an empty folder."""
+    import subprocess
+    import sys
+    code = ("import sys; sys.path.insert(0, %r); import pfb200; pfb200.LIB_PATH = %r\n"
+            "try:\n    pfb200.mask_bytes(100)\nexcept ImportError as e:\n    print('raised', e)\n"
+            % (os.path.join(ROOT, "prime-finder_b200"), str(tmp_path / "libpfb200.so")))
+    out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120).stdout
+    assert out.startswith("raised") and "is missing" in out
