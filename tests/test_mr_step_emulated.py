@@ -1,0 +1,114 @@
+"""The engine's Montgomery step, device code and all, run on the CPU.
+
+tests/cpp/mont_step_emul.cpp compiles prime-finder_b200/csrc/mr_device.cuh
+for the host against a stand-in for the CUDA runtime (tests/cpp/emul/): one
+CTA is THREADS cooperative fibers, __syncthreads a barrier over them, and the
+warp ballots and shuffles exchange values through a barrier over each warp.  The
+engine's own table builders (mr_tables_host.h) and modulus set-up
+(bigint_host.h) feed it.  Each result must equal, limb for limb, Montgomery's
+REDC as the kernel defines it: with R = 2^(22 H), N' = -N^-1 mod R,
+m = (T mod R) N' mod R and U = (T + m N) / R, the step leaves U * a for
+T = x^2 (squaring), T = x y (general product through y's stored spectrum,
+the Lucas test's form) or T = x (conversion out of Montgomery form).
+
+This pins the arithmetic of the transforms, the fused pointwise sweep, the
+zero-padded first pass, the CRT, the carry-lookahead passes and the
+end-around carry at the transform lengths 2^8, 2^9, 2^10, 2^14 (both primes
+in one CTA) and 2^15 (one prime after the other, through the spill buffer).
+It does not stand in for the GPU tests: timing, memory ordering between
+CTAs and the scheduler are not emulated.
+"""
+import os
+import random
+import subprocess
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.set_int_max_str_digits(0)
+LENGTHS = (8, 9, 10, 14, 15)
+
+
+@pytest.fixture(scope="module")
+def emul(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("emul") / "mont_step_emul")
+    subprocess.run(["g++", "-O2", "-std=c++20", "-Wno-unknown-pragmas",
+                    "-I", os.path.join(ROOT, "tests", "cpp", "emul"),
+                    "-I", os.path.join(ROOT, "prime-finder_b200", "csrc"),
+                    "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "mont_step_emul.cpp"), "-o", exe], check=True)
+
+    def run(lines):
+        out = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True,
+                             check=True, timeout=600).stdout.split()
+        assert len(out) == len(lines)
+        return [int(x, 16) for x in out]
+    return run
+
+
+def neg_inv_pow2(N, k):
+    """-N^-1 mod 2^k for odd N (Newton: x <- x (2 - N x), doubling the bits)."""
+    x, bits = 1, 1
+    while bits < k:
+        bits = min(2 * bits, k)
+        x = (x * (2 - N * x)) & ((1 << bits) - 1)
+    return (-x) & ((1 << k) - 1)
+
+
+def redc(logl, N, T, a=1):
+    k = 22 << (logl - 1)  # R = 2^k: reductions by R are masks and shifts
+    mask = (1 << k) - 1
+    m = ((T & mask) * neg_inv_pow2(N, k)) & mask
+    return ((T + m * N) >> k) * a
+
+
+def modulus(rng, logl, abits):
+    """Odd N with R > 4 a^2 N for a of abits bits (the engine's bound)."""
+    H = 1 << (logl - 1)
+    nb = 22 * H - 2 - 2 * abits - rng.randrange(0, 60)
+    return rng.getrandbits(nb) | 1 | (1 << (nb - 1))
+
+
+@pytest.mark.parametrize("logl", LENGTHS)
+def test_squaring_step(emul, logl):
+    rng = random.Random(100 + logl)
+    lines, want = [], []
+    for a in (1, 2, 3, 65535):
+        N = modulus(rng, logl, a.bit_length())
+        for x in (rng.randrange(0, 4 * N), 4 * N - 1, 0, 1):
+            lines.append("step %d %x %x %d" % (logl, N, x, a))
+            want.append(redc(logl, N, x * x, a))
+    assert emul(lines) == want
+
+
+@pytest.mark.parametrize("logl", LENGTHS)
+def test_general_product_and_conversion(emul, logl):
+    rng = random.Random(200 + logl)
+    lines, want = [], []
+    for _ in range(2):
+        N = modulus(rng, logl, 2)
+        x, y = rng.randrange(0, 4 * N), rng.randrange(0, 4 * N)
+        lines.append("mul %d %x %x %x %d" % (logl, N, x, y, 2))
+        want.append(redc(logl, N, x * y, 2))
+        lines.append("redc %d %x %x" % (logl, N, x))
+        want.append(redc(logl, N, x))
+    assert emul(lines) == want
+
+
+def test_montgomery_ladder_equals_pow(emul):
+    """A short square-and-multiply ladder in Montgomery form, fed back through
+    the emulated step, ends at pow(2, e, N): the step composes as the
+    persistent kernel composes it (x0 = R mod N, one step per exponent bit,
+    a final conversion)."""
+    rng = random.Random(7)
+    logl = 9
+    H = 1 << (logl - 1)
+    R = 1 << (22 * H)
+    N = modulus(rng, logl, 2)
+    e = rng.getrandbits(12) | (1 << 11)
+    x = R % N
+    for bit in bin(e)[2:]:
+        x = emul(["step %d %x %x %d" % (logl, N, x, 2 if bit == "1" else 1)])[0]
+    r = emul(["redc %d %x %x" % (logl, N, x)])[0]
+    assert r % N == pow(2, e, N)
