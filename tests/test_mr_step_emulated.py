@@ -112,3 +112,32 @@ def test_montgomery_ladder_equals_pow(emul):
         x = emul(["step %d %x %x %d" % (logl, N, x, 2 if bit == "1" else 1)])[0]
     r = emul(["redc %d %x %x" % (logl, N, x)])[0]
     assert r % N == pow(2, e, N)
+
+
+def test_no_out_of_bounds_access(tmp_path):
+    """Built with AddressSanitizer, the emulated step touches its shared-memory
+    and global buffers (exact-size host arrays here) only within bounds, for
+    every form at every emulated length."""
+    exe = str(tmp_path / "mont_step_emul_asan")
+    cc = subprocess.run(["g++", "-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer", "-std=c++20",
+                         "-Wno-unknown-pragmas",
+                         "-I", os.path.join(ROOT, "tests", "cpp", "emul"),
+                         "-I", os.path.join(ROOT, "prime-finder_b200", "csrc"),
+                         "-I", os.path.join(ROOT, "include"),
+                         os.path.join(ROOT, "tests", "cpp", "mont_step_emul.cpp"), "-o", exe],
+                        capture_output=True, text=True)
+    if cc.returncode != 0 and "asan" in cc.stderr.lower():
+        pytest.skip("no AddressSanitizer runtime: " + cc.stderr.strip().splitlines()[-1])
+    assert cc.returncode == 0, cc.stderr
+    rng = random.Random(3)
+    lines, want = [], []
+    for logl in LENGTHS:
+        N = modulus(rng, logl, 2)
+        x, y = rng.randrange(0, 4 * N), rng.randrange(0, 4 * N)
+        lines += ["step %d %x %x 2" % (logl, N, x), "mul %d %x %x %x 2" % (logl, N, x, y),
+                  "redc %d %x %x" % (logl, N, x)]
+        want += [redc(logl, N, x * x, 2), redc(logl, N, x * y, 2), redc(logl, N, x)]
+    env = dict(os.environ, ASAN_OPTIONS="detect_stack_use_after_return=0:detect_leaks=0")
+    r = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0 and "ERROR: AddressSanitizer" not in r.stderr, r.stderr[-2000:]
+    assert [int(v, 16) for v in r.stdout.split()] == want
