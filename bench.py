@@ -186,6 +186,38 @@ def cpu_sieve_baseline(procs=None, frac=0.05):
                       "one process per core, scaled by prime count" % int(frac * 100)}
 
 
+def odd_primes_below(lim):
+    """Odd primes <= lim by a plain Eratosthenes in numpy (the sieve's input data)."""
+    import numpy as np
+    sieve = np.ones(lim // 2 + 1, dtype=bool)
+    sieve[0] = False
+    for i in range(1, int(lim ** 0.5) // 2 + 1):
+        if sieve[i]:
+            p = 2 * i + 1
+            sieve[p * p // 2::p] = False
+    primes = (2 * np.nonzero(sieve)[0] + 1).astype(np.uint32)
+    return primes[primes <= lim]
+
+
+def sieve_case():
+    """One triple, (50000, 30000, 100), on the 9999 x 9999 grid with every odd
+    prime below 1e8 (the case of the sieve's ncu captures): one untimed call,
+    then one timed with CUDA events."""
+    import torch
+    import pfb200
+    sv = pfb200.Sieve(odd_primes_below(100_000_000), 0)
+    stream = torch.cuda.Stream()
+    dmask = torch.zeros(pfb200.mask_bytes(9999), dtype=torch.uint8, device="cuda")
+    sv.run([(50000, 30000, 100)], 9999, dmask, stream=stream.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sv.run([(50000, 30000, 100)], 9999, dmask, stream=stream.cuda_stream)
+    e1.record(stream)
+    stream.synchronize()
+    print(json.dumps({"case": "sieve K=9999 (50000, 30000, 100), primes < 1e8", "ms": e0.elapsed_time(e1)}))
+    sv.close()
+
+
 # small cases of the squaring kernel for ncu captures: N and rev(N) of four
 # (k, j) at one (a, b, c), 8 candidates (one CTA each), one launch of 64 squarings
 MR_CASES = {
@@ -240,7 +272,12 @@ def main():
     ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
     ap.add_argument("--mr-case", choices=sorted(MR_CASES) + ["all"],
                     help="only run a small case of the squaring kernel (8 candidates, 64 squarings; for ncu)")
+    ap.add_argument("--sieve-case", action="store_true",
+                    help="only run one K = 9999 sieve triple twice (for ncu)")
     args = ap.parse_args()
+    if args.sieve_case:
+        sieve_case()
+        return
     if args.mr_case:
         for name in (sorted(MR_CASES) if args.mr_case == "all" else [args.mr_case]):
             mr_case(name)
@@ -303,16 +340,7 @@ def main():
         return replicas.max_over_ranks(x, dist, "cuda")
 
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    # primes for the sieve: generated by a plain Eratosthenes in numpy (input data)
-    lim = 100_000_000
-    sieve = np.ones(lim // 2 + 1, dtype=bool)
-    sieve[0] = False
-    for i in range(1, int(lim ** 0.5) // 2 + 1):
-        if sieve[i]:
-            p = 2 * i + 1
-            sieve[p * p // 2::p] = False
-    primes = (2 * np.nonzero(sieve)[0] + 1).astype(np.uint32)
-    primes = primes[primes <= lim]
+    primes = odd_primes_below(100_000_000)
 
     # --- sieve -------------------------------------------------------------
     sv = pfb200.Sieve(primes, dev)

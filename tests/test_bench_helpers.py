@@ -25,3 +25,9 @@ def test_mr_cases_are_eight_candidates():
         assert c < b < a
         if pairs is not None:
             assert len(pairs) == 4  # N and rev(N) of each: 8 candidates, one CTA each
+
+
+def test_sieve_input_primes():
+    P = bench.odd_primes_below(1_000_000)
+    assert len(P) == 78497 and P[0] == 3 and P[-1] == 999983  # pi(10^6) = 78498, less the prime 2
+    assert len(bench.odd_primes_below(100)) == 24
