@@ -7,6 +7,13 @@
 
 #include "pfb_sieve.h"
 
+// A kernel's dynamic shared memory as an array of T.  A macro so that a host
+// build of the kernels (the CPU emulation in the tests) can supply its own
+// storage.
+#ifndef PFB_DYNAMIC_SMEM
+#define PFB_DYNAMIC_SMEM(T, name) extern __shared__ T name[]
+#endif
+
 namespace pfb {
 
 // Thread-local last-error text behind pfb_last_error().

@@ -56,583 +56,7 @@ int cuda_fail(cudaError_t e, const char *what, const char *file, int line) {
 
 extern "C" const char *pfb_last_error(void) { return pfb::g_err; }
 
-namespace {
-
-using pfb::Mod32;
-
-constexpr uint32_t kTinyLimit = 512;      // primes below: one warp per (prime,row)
-constexpr int kTileRows = 64;             // rows of the (k,j) grid per shared-memory tile
-constexpr int kBlockTile = 512;
-constexpr int kBlockLarge = 256;
-
-__host__ __device__ inline int ndigits(int x) { return x < 10 ? 1 : x < 100 ? 2 : x < 1000 ? 3 : 4; }
-__host__ __device__ inline uint32_t pow10i(int d) {
-    return d == 0 ? 1u : d == 1 ? 10u : d == 2 ? 100u : d == 3 ? 1000u : 10000u;
-}
-// Decimal reversal of x written with exactly l digits (miller_rabin.c:45-54).
-__device__ __forceinline__ uint32_t rev_digits(uint32_t x, int l) {
-    uint32_t r = 0;
-    for (int i = 0; i < l; i++) {
-        uint32_t q = x / 10u;
-        r = r * 10u + (x - q * 10u);
-        x = q;
-    }
-    return r;
-}
-
-// Shared-memory words of a tile of `rows` grid rows: the bit range may start
-// and end inside a word, hence the two extra words.
-inline size_t tile_smem_bytes(uint32_t rows, int K) {
-    return (((size_t)rows * (size_t)K + 31u) / 32u + 2u) * sizeof(uint32_t);
-}
-
-inline uint32_t small_limit(int K) {
-    uint32_t s = pow10i(ndigits(K));
-    return s > 4096u ? s : 4096u;
-}
-
-// Per (prime, triple) line coefficients.  flags: bit 0 = N form active,
-// bit lk = rev k-class lk active (1..4), bit 4+lj = rev j-class lj active.
-struct LineConsts {
-    uint32_t an, bn;
-    uint32_t ar[4];
-    uint32_t br[4][4];
-    uint32_t flags;
-};
-
-// Small-prime record kept in global memory between the set-up kernel and
-// the tile kernel.
-struct SmallRec {
-    uint32_t p;
-    uint32_t m_lo, m_hi;
-    LineConsts lc;
-};
-
-__device__ void line_consts(const Mod32 &M, long long a, long long b, long long c, LineConsts &s) {
-    const uint32_t p = M.p;
-    const bool inv_ok = (p & 1u) && (p % 5u != 0u);
-    const uint32_t ten = 10u % p;
-    uint32_t inv10 = 0;
-    if (inv_ok) {
-        uint32_t d = p % 10u;
-        uint32_t t = d == 1 ? 9u : d == 3 ? 3u : d == 7 ? 7u : 1u;
-        inv10 = (uint32_t)(((unsigned long long)p * t + 1ull) / 10ull);
-    }
-    // 10^e mod p (e >= 0) and 10^-e mod p (only when 10 is invertible).  When
-    // p is 2 or 5, 10^e is 1 for e == 0 and 0 otherwise, and 1 is its own
-    // inverse: every coefficient below then reduces to 0 or 1 consistently.
-    auto pw = [&](long long e) -> uint32_t { return inv_ok ? M.pow(ten, (unsigned long long)e) : (e == 0 ? 1u : 0u); };
-    auto ipw = [&](long long e) -> uint32_t { return inv_ok ? M.pow(inv10, (unsigned long long)e) : (e == 0 ? 1u : 0u); };
-
-    s.flags = 0;
-    const uint32_t ra = pw(a);
-    const uint32_t ram1 = M.sub(ra, 1u);
-    // N form: j * 10^c == 10^a - 1 - k * 10^b  (trial_div_cpu.c:40-52).
-    if (inv_ok || c == 0) {
-        const uint32_t inv_rc = ipw(c);
-        s.an = M.mul(ram1, inv_rc);
-        s.bn = inv_ok ? (b >= c ? pw(b - c) : ipw(c - b)) : M.mul(pw(b), inv_rc);
-        s.flags |= 1u;
-    } else {
-        s.an = s.bn = 0;
-    }
-    // rev form (trial_div_cpu.c:54-101): rb_rev[l] = 10^(a-b-l), rc_rev[l] = 10^(a-c-l),
-    // a class is skipped when its exponent is negative or its power is 0 mod p.
-    uint32_t rbr[4], irc[4];
-    {
-        const long long e4 = a - b - 4;
-        uint32_t base = e4 >= 0 ? pw(e4) : 0u;
-        for (int l = 4; l >= 1; l--) {
-            const long long e = a - b - l;
-            const bool ok = e >= 0 && (inv_ok || e == 0);
-            if (ok) {
-                rbr[l - 1] = (e4 >= 0) ? base : pw(e);
-                s.flags |= 1u << l;
-            } else {
-                rbr[l - 1] = 0;
-            }
-            if (e4 >= 0) base = M.mul(base, ten);
-        }
-    }
-    {
-        const long long f1 = a - c - 1;
-        uint32_t q = (inv_ok && f1 >= 0) ? ipw(f1) : 0u;
-        for (int l = 1; l <= 4; l++) {
-            const long long e = a - c - l;
-            const bool ok = e >= 0 && (inv_ok || e == 0);
-            if (ok) {
-                irc[l - 1] = inv_ok ? q : 1u;
-                s.flags |= 1u << (4 + l);
-            } else {
-                irc[l - 1] = 0;
-            }
-            if (inv_ok) q = M.mul(q, ten);
-        }
-    }
-    for (int lj = 0; lj < 4; lj++) {
-        s.ar[lj] = M.mul(ram1, irc[lj]);
-        for (int lk = 0; lk < 4; lk++) s.br[lk][lj] = M.mul(rbr[lk], irc[lj]);
-    }
-}
-
-__device__ __forceinline__ void mark_global(uint32_t *mask, int K, uint32_t k, uint32_t j) {
-    const uint32_t q = (k - 1u) * (uint32_t)K + (j - 1u);
-    atomicOr(mask + (q >> 5), 1u << (q & 31u));
-}
-
-// ---------------------------------------------------------------------------
-// Lattice enumeration of one line.  The hits of y == A - B x (mod p) with x in
-// [x0, x1] and 1 <= y <= Y (Y < p) are the points of a translate of the
-// lattice {(i, t) : i == g t (mod p)}, g = -B, that fall in the strip
-// 0 <= i < Y (i = y - 1, t = x - x0).
-//
-//  * first_hit: the smallest t >= 0 with (c + g t) mod p < Y, by a Euclid-like
-//    descent on (multiplier, modulus) that halves the modulus every level
-//    (reflection keeps the multiplier below half the modulus): depth <= 33.
-//  * fk_reduce: a basis u = (-a, beta), v = (c, delta) with 0 <= a, c < Y,
-//    a + c >= Y, beta, delta > 0 (Franke and Kleinjung, "Continued fractions
-//    and lattice sieving", 2005).  From a strip point (i, t) the next strip
-//    point is (i, t) + u if i >= a, + v if i + c < Y, else + u + v.
-// Cost: O(log p) per line plus O(1) per hit, where walking the K values of x
-// costs O(K).
-
-// Exact quotients by d from a double estimate (rd = 1/d, one division per
-// divisor) corrected with integer arithmetic: for quotients below 2^50 the
-// estimate is within two units.
-__device__ __forceinline__ uint32_t quot32(uint32_t v, uint32_t d, double rd) {
-    uint32_t q = (uint32_t)((double)v * rd);
-    long long r = (long long)v - (long long)q * d;
-    while (r < 0) {
-        q--;
-        r += d;
-    }
-    while (r >= (long long)d) {
-        q++;
-        r -= d;
-    }
-    return q;
-}
-
-__device__ __forceinline__ unsigned long long quot64(unsigned long long n, uint32_t d, double rd) {
-    unsigned long long q = (unsigned long long)((double)n * rd);
-    long long r = (long long)(n - q * d);
-    while (r < 0) {
-        q--;
-        r += d;
-    }
-    while (r >= (long long)d) {
-        q++;
-        r -= d;
-    }
-    return q;
-}
-
-// The descent keeps, per level, the multiplier a, its reciprocal and the
-// interval start L; the level's modulus is the previous level's multiplier
-// (p at level 0).
-__device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, uint32_t Y) {
-    if (c < Y) return 0u;
-    uint32_t a = g, m = p, L = p - c, R = p - c + Y - 1u;
-    uint32_t sa[34], sl[34];
-    double sr[34];
-    int d = 0;
-    uint32_t x;
-    for (;;) {
-        const double rd = 1.0 / (double)a;
-        const uint32_t k = quot32(L - 1u, a, rd) + 1u;  // ceil(L / a), L >= 1
-        if ((unsigned long long)a * k <= R) {
-            x = k;
-            break;
-        }
-        if (d >= 34) return 0xFFFFFFFFu;  // unreachable: the modulus halves each level
-        sa[d] = a;
-        sl[d] = L;
-        sr[d] = rd;
-        d++;
-        const uint32_t r = m - quot32(m, a, rd) * a;  // != 0: gcd(a, m) = 1 along the chain
-        uint32_t a2 = a - r, L2 = L - quot32(L, a, rd) * a, R2 = R - quot32(R, a, rd) * a;
-        const uint32_t m2 = a;
-        if (a2 > (m2 >> 1)) {               // reflect: a x in [L, R] <=> (m - a) x in [m - R, m - L]
-            a2 = r;
-            const uint32_t t2 = m2 - R2;
-            R2 = m2 - L2;
-            L2 = t2;
-        }
-        a = a2;
-        m = m2;
-        L = L2;
-        R = R2;
-    }
-    while (d > 0) {
-        d--;
-        const uint32_t md = d ? sa[d - 1] : p;
-        x = (uint32_t)quot64((unsigned long long)x * md + sl[d] + sa[d] - 1u, sa[d], sr[d]);  // ceil
-    }
-    return x;
-}
-
-struct FKBasis {
-    uint32_t a, beta, c, delta;
-};
-
-__device__ __noinline__ FKBasis fk_reduce(uint32_t g, uint32_t p, uint32_t I) {
-    uint32_t a = p, beta = 0u, c = g, delta = 1u;
-    for (;;) {
-        if (c < I) {
-            const uint32_t k = (a - (I - c)) / c;
-            a -= k * c;
-            beta += k * delta;
-            break;
-        }
-        if (a < I) {
-            const uint32_t k = (c - (I - a)) / a;
-            c -= k * a;
-            delta += k * beta;
-            break;
-        }
-        if (a >= c) {
-            const uint32_t k = a / c;
-            a -= k * c;
-            beta += k * delta;
-        } else {
-            const uint32_t k = c / a;
-            c -= k * a;
-            delta += k * beta;
-        }
-    }
-    return FKBasis{a, beta, c, delta};
-}
-
-// Calls visit(x, y) for every x in [x0, x1] with y = (A - B x) mod p in
-// [1, Y]; requires 1 <= Y < p, B != 0 (mod p), x1 - x0 < p.
-template <class Visit>
-__device__ __forceinline__ void line_hits(const Mod32 &M, uint32_t A, uint32_t B, uint32_t x0, uint32_t x1,
-                                          uint32_t Y, Visit visit) {
-    const uint32_t p = M.p;
-    const uint32_t g = p - B;
-    const uint32_t c0 = M.sub(M.sub(A, 1u % p), M.mul(B, x0 % p));  // (A - 1 - B x0) mod p
-    unsigned long long t = first_hit(c0, g, p, Y);
-    const unsigned long long span = (unsigned long long)(x1 - x0);
-    if (t > span) return;
-    const FKBasis fb = fk_reduce(g, p, Y);
-    uint32_t i = M.red((unsigned long long)g * t + c0);
-    while (t <= span) {
-        visit(x0 + (uint32_t)t, i + 1u);
-        if (i >= fb.a) {
-            i -= fb.a;
-            t += fb.beta;
-        } else if (i + fb.c < Y) {
-            i += fb.c;
-            t += fb.delta;
-        } else {
-            i = i - fb.a + fb.c;
-            t += (unsigned long long)fb.beta + fb.delta;
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
-// Prime-list split: tiny (p < 512), small (512 <= p < S); large primes are
-// filtered inside the large-prime kernel.
-// A list with repeated entries can exceed `cap`; the excess is counted but
-// not stored, and the host rejects the list.
-__global__ void split_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
-                             uint32_t cap, uint32_t *tiny, uint32_t *small, uint32_t *counts) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t p = primes[i];
-        if (p < 2u || p >= s_limit) continue;
-        if (p < kTinyLimit) {
-            const uint32_t at = atomicAdd(&counts[0], 1u);
-            if (at < cap) tiny[at] = p;
-        } else {
-            const uint32_t at = atomicAdd(&counts[1], 1u);
-            if (at < cap) small[at] = p;
-        }
-    }
-}
-
-// Set-up of the small-prime records for every triple: rec[t * cap + i];
-// cap = 2 * capacity of each list.
-__global__ void small_setup_kernel(const uint32_t *__restrict__ tiny, const uint32_t *__restrict__ small,
-                                   const uint32_t *__restrict__ counts, const long long *__restrict__ abc,
-                                   int n_abc, uint32_t cap, SmallRec *__restrict__ rec) {
-    const uint32_t n_tiny = min(counts[0], cap / 2u), n_small = min(counts[1], cap / 2u);
-    const uint32_t n = n_tiny + n_small;
-    const int t = blockIdx.y;
-    if (t >= n_abc) return;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t p = i < n_tiny ? tiny[i] : small[i - n_tiny];
-        Mod32 M;
-        M.init(p);
-        SmallRec r;
-        r.p = p;
-        r.m_lo = (uint32_t)M.m;
-        r.m_hi = (uint32_t)(M.m >> 32);
-        line_consts(M, abc[3 * t], abc[3 * t + 1], abc[3 * t + 2], r.lc);
-        rec[(size_t)t * cap + i] = r;
-    }
-}
-
-// Marks of one (prime,row) item.  Lanes lane0, lane0+step, ... of the hit
-// sequences are handled by this thread (step = 32 for warp items, 1 for
-// thread items).
-__device__ __forceinline__ void small_item(const SmallRec &r, uint32_t k, int K, uint32_t lane0,
-                                           uint32_t step, uint32_t *tile, uint32_t bit_base) {
-    Mod32 M;
-    M.p = r.p;
-    M.m = ((unsigned long long)r.m_hi << 32) | r.m_lo;
-    const uint32_t p = r.p;
-    const LineConsts &lc = r.lc;
-    auto mark = [&](uint32_t j) {
-        const uint32_t q = (k - 1u) * (uint32_t)K + (j - 1u) - bit_base;
-        atomicOr(tile + (q >> 5), 1u << (q & 31u));
-    };
-    if (lc.flags & 1u) {
-        uint32_t j0 = M.sub(lc.an, M.mul(k % p, lc.bn));
-        if (j0 == 0) j0 = p;
-        for (unsigned long long j = j0 + (unsigned long long)lane0 * p; j <= (unsigned long long)K;
-             j += (unsigned long long)step * p)
-            mark((uint32_t)j);
-    }
-    const int lk = ndigits((int)k);
-    if (!(lc.flags & (1u << lk))) return;
-    const uint32_t rk = rev_digits(k, lk) % p;
-    const int maxd = ndigits(K);
-    for (int lj = 1; lj <= maxd; lj++) {
-        if (!(lc.flags & (1u << (4 + lj)))) continue;
-        const uint32_t lim = pow10i(lj);  // rj < lim
-        uint32_t t0 = M.sub(lc.ar[lj - 1], M.mul(rk, lc.br[lk - 1][lj - 1]));
-        if (t0 == 0) t0 = p;
-        for (unsigned long long rj = t0 + (unsigned long long)lane0 * p; rj < lim;
-             rj += (unsigned long long)step * p) {
-            const uint32_t r32 = (uint32_t)rj;
-            if (lj > 1 && r32 % 10u == 0u) continue;  // j would have fewer digits
-            const uint32_t j = rev_digits(r32, lj);
-            if (j <= (uint32_t)K) mark(j);
-        }
-    }
-}
-
-// Row-tile sieve of the small primes.  grid = (tiles, triples).
-__global__ void __launch_bounds__(kBlockTile)
-small_tile_kernel(const SmallRec *__restrict__ rec, const uint32_t *__restrict__ counts, uint32_t cap,
-                  int K, uint32_t *__restrict__ mask, size_t words_per_triple) {
-    extern __shared__ uint32_t tile[];
-    const int t = blockIdx.y;
-    const uint32_t k0 = 1u + blockIdx.x * kTileRows;
-    if (k0 > (uint32_t)K) return;
-    const uint32_t k1 = min((uint32_t)K + 1u, k0 + kTileRows);
-    const uint32_t rows = k1 - k0;
-    const uint32_t bit_lo = (k0 - 1u) * (uint32_t)K;
-    const uint32_t bit_hi = (k1 - 1u) * (uint32_t)K;
-    const uint32_t w0 = bit_lo >> 5, w1 = (bit_hi - 1u) >> 5;
-    const uint32_t nw = w1 - w0 + 1u;
-    for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) tile[w] = 0u;
-    __syncthreads();
-
-    const uint32_t n_tiny = min(counts[0], cap / 2u), n_small = min(counts[1], cap / 2u);
-    const SmallRec *rt = rec + (size_t)t * cap;
-    const uint32_t bit_base = w0 << 5;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-
-    // Tiny primes: one warp per (prime,row), lanes share the hits.
-    for (uint32_t it = warp; it < n_tiny * rows; it += nwarps) {
-        const SmallRec r = rt[it / rows];
-        small_item(r, k0 + it % rows, K, lane, 32u, tile, bit_base);
-    }
-    // Other small primes: one thread per (prime,row).
-    for (uint32_t it = threadIdx.x; it < n_small * rows; it += blockDim.x) {
-        const SmallRec r = rt[n_tiny + it / rows];
-        small_item(r, k0 + it % rows, K, 0u, 1u, tile, bit_base);
-    }
-    __syncthreads();
-    uint32_t *g = mask + (size_t)t * words_per_triple + w0;
-    for (uint32_t w = threadIdx.x; w < nw; w += blockDim.x) {
-        const uint32_t v = tile[w];
-        if (v) atomicOr(g + w, v);
-    }
-}
-
-// Large primes (p >= S > K): each line meets every row at most once.  One
-// thread per prime; incremental updates replace the multiplications.
-__global__ void __launch_bounds__(kBlockLarge)
-large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
-             const long long *__restrict__ abc, int K, uint32_t *__restrict__ mask,
-             size_t words_per_triple) {
-    const int t = blockIdx.y;
-    const long long a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
-    uint32_t *m = mask + (size_t)t * words_per_triple;
-    const int maxd = ndigits(K);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t p = primes[i];
-        if (p < s_limit) continue;
-        Mod32 M;
-        M.init(p);
-        LineConsts lc;
-        line_consts(M, a, b, c, lc);
-
-        if (lc.flags & 1u)  // N form: j == AN - k BN (p > K: at most one j per k)
-            line_hits(M, lc.an, lc.bn, 1u, (uint32_t)K, (uint32_t)K,
-                      [&](uint32_t k, uint32_t j) { mark_global(m, K, k, j); });
-        for (int lk = 1; lk <= maxd; lk++) {  // rev form, per digit class of k
-            if (!(lc.flags & (1u << lk))) continue;
-            const uint32_t lo = pow10i(lk - 1), hi = pow10i(lk) - 1u;
-            // State of the four j classes in registers.  A class that is off
-            // (no such digit count on the grid, or skipped by the reference's
-            // rules) keeps value 0 and step 0: 0 never passes the hit test.
-            uint32_t tv[4], st[4], on = 0u;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const bool c_on = (q + 1 <= maxd) && (lc.flags & (1u << (5 + q)));
-                on |= c_on ? (1u << q) : 0u;
-                st[q] = c_on ? lc.br[lk - 1][q] : 0u;
-                tv[q] = c_on ? lc.ar[q] : 0u;
-            }
-            if (hi <= (uint32_t)K && lk >= 3) {
-                // Long class (rev(k) takes up to 9999 values): per j class, a
-                // lattice walk when rev(j) has >= 3 digits; otherwise iterate
-                // the <= 99 values of rev(j): rev(k) == (AR - rev(j)) BR^-1,
-                // BR^-1 = 10^(b-c+lk-lj) = BN * 10^(lk-lj).  (Not unrolled:
-                // the walk is large and the instruction cache small.)
-#pragma unroll 1
-                for (int q = 0; q < 4; q++) {
-                    if (!(on & (1u << q))) continue;
-                    const int lj = q + 1;
-                    const uint32_t ylim = pow10i(lj) - 1u;
-                    if (lj >= 3) {
-                        line_hits(M, lc.ar[q], st[q], 1u, hi, ylim, [&](uint32_t rk, uint32_t rj) {
-                            if (rk % 10u != 0u && rj % 10u != 0u) {
-                                const uint32_t j = rev_digits(rj, lj);
-                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
-                            }
-                        });
-                    } else {
-                        const uint32_t inv = M.mul(lc.bn, pow10i(lk - lj) % p);
-                        uint32_t rk = M.mul(lc.ar[q], inv);  // rev(j) = 0
-                        for (uint32_t rj = 1; rj <= ylim; rj++) {
-                            rk = M.sub(rk, inv);
-                            if (rk - 1u < hi && rk % 10u != 0u && (lj == 1 || rj % 10u != 0u)) {
-                                const uint32_t j = rev_digits(rj, lj);
-                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
-                            }
-                        }
-                    }
-                }
-            } else if (hi <= (uint32_t)K) {
-                // short class (lk <= 2): walk rev(k) = 1 .. hi linearly
-#pragma unroll
-                for (int q = 0; q < 4; q++) tv[q] = M.sub(tv[q], st[q]);  // rk = 1
-                for (uint32_t rk = 1; rk <= hi; rk++) {
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (tv[q] - 1u < pow10i(q + 1) - 1u) {  // 1 <= rev(j) < 10^(q+1)
-                            const uint32_t rj = tv[q];
-                            if ((lk == 1 || rk % 10u != 0u) && (q == 0 || rj % 10u != 0u)) {
-                                const uint32_t j = rev_digits(rj, q + 1);
-                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
-                            }
-                        }
-                        tv[q] = M.sub(tv[q], st[q]);
-                    }
-                }
-            } else {
-                // partial top class (K < 10^lk - 1): visit the k on the grid directly
-                for (uint32_t k = lo; k <= (uint32_t)K; k++) {
-                    const uint32_t rk = rev_digits(k, lk) % p;
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (!(on & (1u << q))) continue;
-                        const uint32_t rj = M.sub(lc.ar[q], M.mul(rk, st[q]));
-                        if (rj - 1u < pow10i(q + 1) - 1u && (q == 0 || rj % 10u != 0u)) {
-                            const uint32_t j = rev_digits(rj, q + 1);
-                            if (j <= (uint32_t)K) mark_global(m, K, k, j);
-                        }
-                    }
-                }
-            }
-        }
-    }
-}
-
-// Survivor compaction, pass 1: zero bits per 1024-bit chunk.
-__global__ void surv_count_kernel(const uint32_t *__restrict__ mask, uint32_t nbits, uint32_t *chunk_cnt) {
-    const uint32_t w = blockIdx.x * 32u + threadIdx.x;
-    uint32_t c = 0;
-    if (w * 32u < nbits) {
-        uint32_t v = ~mask[w];
-        const uint32_t rem = nbits - w * 32u;
-        if (rem < 32u) v &= (1u << rem) - 1u;
-        c = __popc(v);
-    }
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31u) == 0u) chunk_cnt[blockIdx.x] = c;
-}
-
-// Pass 2: exclusive scan of the chunk counts (single block).
-__global__ void surv_scan_kernel(uint32_t *chunk_cnt, uint32_t n, uint32_t *total) {
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (uint32_t base = 0; base < n; base += blockDim.x) {
-        const uint32_t i = base + threadIdx.x;
-        const uint32_t v = i < n ? chunk_cnt[i] : 0u;
-        // block-wide inclusive scan (warp shuffles + smem)
-        __shared__ uint32_t wsum[32];
-        uint32_t x = v;
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-            if ((threadIdx.x & 31u) >= (uint32_t)o) x += y;
-        }
-        if ((threadIdx.x & 31u) == 31u) wsum[threadIdx.x >> 5] = x;
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            uint32_t s = threadIdx.x < (blockDim.x >> 5) ? wsum[threadIdx.x] : 0u;
-            for (int o = 1; o < 32; o <<= 1) {
-                const uint32_t y = __shfl_up_sync(0xffffffffu, s, o);
-                if (threadIdx.x >= (uint32_t)o) s += y;
-            }
-            wsum[threadIdx.x] = s;
-        }
-        __syncthreads();
-        const uint32_t wpre = (threadIdx.x >> 5) ? wsum[(threadIdx.x >> 5) - 1] : 0u;
-        const uint32_t incl = x + wpre;
-        if (i < n) chunk_cnt[i] = carry + incl - v;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry += incl;
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) *total = carry;
-}
-
-// Pass 3: write (k << 16 | j) of every zero bit in k-major order.
-__global__ void surv_write_kernel(const uint32_t *__restrict__ mask, uint32_t nbits, int K,
-                                  const uint32_t *__restrict__ chunk_off, uint32_t *out, uint32_t cap) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t w = blockIdx.x * 32u + lane;
-    uint32_t v = 0;
-    if (w * 32u < nbits) {
-        v = ~mask[w];
-        const uint32_t rem = nbits - w * 32u;
-        if (rem < 32u) v &= (1u << rem) - 1u;
-    }
-    const uint32_t c = __popc(v);
-    uint32_t pre = c;
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xffffffffu, pre, o);
-        if (lane >= (uint32_t)o) pre += y;
-    }
-    uint32_t pos = chunk_off[blockIdx.x] + pre - c;
-    while (v) {
-        const uint32_t bit = __ffs(v) - 1u;
-        v &= v - 1u;
-        const uint32_t q = w * 32u + bit;
-        const uint32_t k = q / (uint32_t)K + 1u, j = q % (uint32_t)K + 1u;
-        if (pos < cap) out[pos] = (k << 16) | j;
-        pos++;
-    }
-}
-
-}  // namespace
+#include "sieve_device.cuh"
 
 // ============================================================================
 // Host side

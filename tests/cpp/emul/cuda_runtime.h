@@ -1,10 +1,11 @@
 // Host stand-in for <cuda_runtime.h>, for running the engine's device code
-// (mr_device.cuh) on the CPU in the tests.  One CTA is emulated by THREADS
-// cooperative fibers on one host thread (ucontext): __syncthreads waits at a
-// barrier over all of them, and the warp-level intrinsics exchange values
-// through a barrier over the 32 fibers of the warp; a fiber that waits
-// switches to the next one, round-robin.  Only what mr_device.cuh uses is
-// provided.
+// (mr_device.cuh, sieve_device.cuh) on the CPU in the tests.  One CTA is
+// emulated by cooperative fibers on one host thread (ucontext), one per CUDA
+// thread: __syncthreads waits at a barrier over all of them, and the
+// warp-level intrinsics exchange values through a barrier over the 32 fibers
+// of the warp; a fiber that waits switches to the next one, round-robin.  A
+// grid runs its CTAs one after another, so atomics need no locking.  Only
+// what those headers use is provided.
 #pragma once
 #include <stdint.h>
 #include <stdlib.h>
@@ -19,8 +20,17 @@
 
 #define __device__
 #define __host__
+#define __global__
 #define __forceinline__ inline
+#define __noinline__ __attribute__((noinline))
+#define __launch_bounds__(...)
 #define __constant__
+#define __shared__ static  // one CTA at a time: a static is the CTA's shared variable
+#define __align__(n) alignas(n)
+#define PFB_DYNAMIC_SMEM(T, name) T *name = emu::dynamic_smem<T>()
+
+typedef int cudaError_t;
+enum : int { cudaSuccess = 0 };
 
 struct uint4 {
     unsigned x, y, z, w;
@@ -30,9 +40,11 @@ struct emu_dim3 {
     unsigned x = 0, y = 0, z = 0;
 };
 
-// The running fiber's indices (set on every switch).
+// The running fiber's indices (set on every switch) and the grid's.
 inline emu_dim3 threadIdx;
 inline emu_dim3 blockDim;
+inline emu_dim3 blockIdx;
+inline emu_dim3 gridDim;
 
 namespace emu {
 
@@ -46,6 +58,12 @@ struct Group {
     int size = 0, arrived = 0;
     unsigned long long gen = 0;
 };
+
+// Dynamic shared memory of the running grid: exactly the bytes the launch
+// asked for (so that a sanitizer sees an overrun).
+inline unsigned char *dyn_smem = nullptr;
+template <class T>
+inline T *dynamic_smem() { return reinterpret_cast<T *>(dyn_smem); }
 
 inline std::vector<Fiber> *fibers = nullptr;
 inline std::vector<Group> *groups = nullptr;  // 0: the CTA; 1 + w: warp w
@@ -116,10 +134,15 @@ inline void run_cta(int threads, const std::function<void()> &f) {
     body = &f;
     blockDim.x = (unsigned)threads;
     const size_t stack_bytes = 256 * 1024;
+    static std::vector<void *> stacks;  // reused by every CTA of the process
+    while ((int)stacks.size() < threads) {
+        void *st = malloc(stack_bytes);
+        if (!st) throw std::runtime_error("fiber stack");
+        stacks.push_back(st);
+    }
     for (int t = 0; t < threads; t++) {
         Fiber &fb = fs[t];
-        fb.stack = malloc(stack_bytes);
-        if (!fb.stack) throw std::runtime_error("fiber stack");
+        fb.stack = stacks[t];
         getcontext(&fb.ctx);
         fb.ctx.uc_stack.ss_sp = fb.stack;
         fb.ctx.uc_stack.ss_size = stack_bytes;
@@ -129,16 +152,60 @@ inline void run_cta(int threads, const std::function<void()> &f) {
     current = 0;
     threadIdx.x = 0;
     swapcontext(&main_ctx, &fs[0].ctx);
-    for (auto &fb : fs) free(fb.stack);
     fibers = nullptr;
     groups = nullptr;
     lane_vals = nullptr;
     body = nullptr;
 }
 
+// Runs f for every thread of a gx x gy grid of CTAs of `threads` threads,
+// one CTA after another, with smem bytes of dynamic shared memory.
+inline void run_grid(unsigned gx, unsigned gy, int threads, const std::function<void()> &f, size_t smem = 0) {
+    std::vector<unsigned char> buf(smem);
+    dyn_smem = smem ? buf.data() : nullptr;
+    gridDim.x = gx;
+    gridDim.y = gy;
+    for (unsigned y = 0; y < gy; y++)
+        for (unsigned x = 0; x < gx; x++) {
+            blockIdx.x = x;
+            blockIdx.y = y;
+            run_cta(threads, f);
+        }
+    dyn_smem = nullptr;
+}
+
 }  // namespace emu
 
 inline void __syncthreads() { emu::group_wait(0); }
+
+inline unsigned atomicOr(unsigned *p, unsigned v) {
+    const unsigned o = *p;
+    *p = o | v;
+    return o;
+}
+
+inline unsigned atomicAdd(unsigned *p, unsigned v) {
+    const unsigned o = *p;
+    *p = o + v;
+    return o;
+}
+
+// CUDA's integer min/max (mixed operands convert as in arithmetic).
+template <class A, class B>
+inline auto min(A a, B b) -> decltype(a + b) {
+    return a < b ? a : b;
+}
+template <class A, class B>
+inline auto max(A a, B b) -> decltype(a + b) {
+    return a < b ? b : a;
+}
+
+inline int __popc(unsigned v) { return __builtin_popcount(v); }
+inline int __ffs(int v) { return __builtin_ffs(v); }
+
+inline unsigned long long __umul64hi(unsigned long long a, unsigned long long b) {
+    return (unsigned long long)(((unsigned __int128)a * b) >> 64);
+}
 
 inline unsigned __umulhi(unsigned a, unsigned b) { return (unsigned)(((unsigned long long)a * b) >> 32); }
 
@@ -155,6 +222,16 @@ inline unsigned __ballot_sync(unsigned, int pred) {
     emu::group_wait(1 + (int)w);
     unsigned r = 0;
     for (unsigned i = 0; i < 32 && base + i < blockDim.x; i++) r |= ((*emu::lane_vals)[base + i] ? 1u : 0u) << i;
+    emu::group_wait(1 + (int)w);
+    return r;
+}
+
+template <class T>
+inline T __shfl_xor_sync(unsigned, T v, int lane_mask) {
+    const unsigned t = threadIdx.x, w = t >> 5, lane = t & 31u;
+    (*emu::lane_vals)[t] = (unsigned long long)v;
+    emu::group_wait(1 + (int)w);
+    const T r = (T)(*emu::lane_vals)[(w << 5) + (lane ^ (unsigned)lane_mask)];
     emu::group_wait(1 + (int)w);
     return r;
 }

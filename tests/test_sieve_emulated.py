@@ -1,0 +1,105 @@
+"""The Phase-1 sieve kernels, device code and all, run on the CPU.
+
+tests/cpp/sieve_emul.cpp compiles prime-finder_b200/csrc/sieve_device.cuh for
+the host against the stand-in CUDA runtime of tests/cpp/emul/ (each CTA as
+cooperative fibers, the CTAs of a grid one after another) and makes the
+launches pfb_sieve_run and pfb_sieve_survivors make for one triple: the
+prime-list split, the small-prime line records and shared-memory row tiles,
+the large-prime lattice walk, and the survivor compaction.  The mask must be
+bit-identical to the oracle's restatement of the reference's trial_div_cpu
+(trial_div_cpu.c:32-111, any K) and the survivor list (compared through its
+count and FNV-1a hash) its zero bits in k-major order; built with
+AddressSanitizer, every access to the mask, the lists, the records and the
+tile's shared memory must stay in bounds.
+"""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import primes_below
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+SRC = os.path.join(ROOT, "tests", "cpp", "sieve_emul.cpp")
+INC = ["-I", os.path.join(ROOT, "tests", "cpp", "emul"), "-I", os.path.join(ROOT, "prime-finder_b200", "csrc"),
+       "-I", os.path.join(ROOT, "include")]
+
+
+def _build(path, asan=False):
+    flags = ["-O1", "-g", "-fsanitize=address", "-fno-omit-frame-pointer"] if asan else ["-O2"]
+    return subprocess.run(["g++"] + flags + ["-std=c++20", "-Wno-unknown-pragmas"] + INC + [SRC, "-o", path],
+                          capture_output=True, text=True)
+
+
+@pytest.fixture(scope="module")
+def emul(tmp_path_factory):
+    exe = str(tmp_path_factory.mktemp("sieve_emul") / "sieve_emul")
+    cc = _build(exe)
+    assert cc.returncode == 0, cc.stderr
+    return exe
+
+
+def _run(exe, P, a, b, c, K, env=None):
+    inp = "%d %d %d %d\n%d %s\n" % (K, a, b, c, len(P), " ".join(map(str, P)))
+    r = subprocess.run([exe], input=inp, capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    first, second = r.stdout.split("\n")[:2]
+    got = bytes.fromhex(first)
+    got = np.frombuffer(got, dtype=">u4").astype("<u4").tobytes()  # words were printed big-endian
+    count, h = map(int, second.split())
+    return got, count, h, r.stderr
+
+
+def _fnv1a64(data: bytes) -> int:
+    h = 1469598103934665603
+    for byte in data:
+        h = ((h ^ byte) * 1099511628211) & 0xFFFFFFFFFFFFFFFF
+    return h
+
+
+def _check(got, count, h, P, a, b, c, K):
+    want = oracle.sieve_grid(np.asarray(P, dtype=np.uint32), a, b, c, K)
+    assert got[:len(want)] == bytes(want), (a, b, c, K)
+    bits = np.unpackbits(np.frombuffer(bytes(want), dtype=np.uint8), bitorder="little")[:K * K].reshape(K, K)
+    k, j = np.nonzero(bits == 0)
+    expect = (((k + 1) << 16) | (j + 1)).astype("<u4")
+    assert count == len(expect)
+    if len(expect) <= 200_000:
+        assert h == _fnv1a64(expect.tobytes())
+
+
+P5 = [p for p in primes_below(100_000).tolist() if p > 2]
+CASES = [(60, 40, 20, 40), (50000, 30000, 100, 100), (181, 9, 3, 150), (101, 60, 0, 64),
+         (120, 70, 30, 1000), (7, 5, 0, 100)]
+
+
+@pytest.mark.parametrize("a,b,c,K", CASES)
+def test_emulated_sieve_equals_oracle(emul, a, b, c, K):
+    _check(*_run(emul, P5, a, b, c, K)[:3], P5, a, b, c, K)
+
+
+def test_emulated_sieve_four_digit_classes(emul):
+    """K = 1200: k and j of 1 to 4 digits (every digit-count class)."""
+    _check(*_run(emul, P5, 50000, 30000, 100, 1200)[:3], P5, 50000, 30000, 100, 1200)
+
+
+def test_emulated_sieve_full_grid(emul):
+    """K = 9999, the largest grid the engine takes (mask and survivor count)."""
+    P = [p for p in primes_below(20_000).tolist() if p > 2]
+    _check(*_run(emul, P, 50000, 30000, 100, 9999)[:3], P, 50000, 30000, 100, 9999)
+
+
+def test_emulated_sieve_in_bounds(tmp_path):
+    exe = str(tmp_path / "sieve_emul_asan")
+    cc = _build(exe, asan=True)
+    if cc.returncode != 0 and "asan" in cc.stderr.lower():
+        pytest.skip("no AddressSanitizer runtime")
+    assert cc.returncode == 0, cc.stderr
+    env = dict(os.environ, ASAN_OPTIONS="detect_stack_use_after_return=0:detect_leaks=0")
+    for a, b, c, K in [(50000, 30000, 100, 100), (181, 9, 3, 150), (120, 70, 30, 1000)]:
+        got, count, surv, err = _run(exe, P5, a, b, c, K, env=env)
+        assert "ERROR: AddressSanitizer" not in err
+        _check(got, count, surv, P5, a, b, c, K)
