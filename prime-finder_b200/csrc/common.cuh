@@ -7,11 +7,11 @@
 
 #include "pfb_sieve.h"
 
-// A kernel's dynamic shared memory as an array of T.  A macro so that a host
-// build of the kernels (the CPU emulation in the tests) can supply its own
-// storage.
+// A kernel's dynamic shared memory as a 16-byte-aligned array of T.  A macro
+// so that a host build of the kernels (the CPU emulation in the tests) can
+// supply its own storage.
 #ifndef PFB_DYNAMIC_SMEM
-#define PFB_DYNAMIC_SMEM(T, name) extern __shared__ T name[]
+#define PFB_DYNAMIC_SMEM(T, name) extern __shared__ __align__(16) T name[]
 #endif
 
 namespace pfb {

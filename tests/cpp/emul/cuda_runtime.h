@@ -190,6 +190,30 @@ inline unsigned atomicAdd(unsigned *p, unsigned v) {
     return o;
 }
 
+inline int atomicCAS(int *p, int cmp, int v) {
+    const int o = *p;
+    if (o == cmp) *p = v;
+    return o;
+}
+
+inline int atomicExch(int *p, int v) {
+    const int o = *p;
+    *p = v;
+    return o;
+}
+
+inline void __threadfence() {}
+
+// Barrier of the CTA that also returns whether pred holds on every thread.
+inline int __syncthreads_and(int pred) {
+    (*emu::lane_vals)[threadIdx.x] = pred ? 1ull : 0ull;
+    emu::group_wait(0);
+    int all = 1;
+    for (unsigned t = 0; t < blockDim.x; t++) all &= (*emu::lane_vals)[t] ? 1 : 0;
+    emu::group_wait(0);
+    return all;
+}
+
 // CUDA's integer min/max (mixed operands convert as in arithmetic).
 template <class A, class B>
 inline auto min(A a, B b) -> decltype(a + b) {
