@@ -3,12 +3,15 @@
 // launches are those pfb_sieve_run and pfb_sieve_survivors make for one
 // triple (sieve.cu: ensure_split, enqueue_sieve, pfb_sieve_survivors).
 //
-// Input: "K a b c", then "n p_1 ... p_n" (the prime list).  Output: the mask
-// as hexadecimal little-endian words (one line), then the number of
-// survivors and the 64-bit FNV-1a hash of the survivor list (k<<16|j as
-// little-endian uint32), in decimal (one line).
+// Input: "K a b c [compact]", then "n p_1 ... p_n" (the prime list).
+// Output: the mask as hexadecimal little-endian words (one line), then the
+// number of survivors and the 64-bit FNV-1a hash of the survivor list
+// (k<<16|j as little-endian uint32), in decimal (one line; "0 0" when
+// compact is given as 0 and the compaction is skipped).
 #include <functional>
 #include <iostream>
+#include <sstream>
+#include <string>
 #include <vector>
 
 #include "sieve_device.cuh"
@@ -17,7 +20,13 @@ int main() {
     int K = 0;
     long long abc[3] = {0, 0, 0};
     uint32_t n = 0;
-    std::cin >> K >> abc[0] >> abc[1] >> abc[2] >> n;
+    std::string first;
+    std::getline(std::cin, first);
+    std::istringstream f(first);
+    int compact = 1;
+    f >> K >> abc[0] >> abc[1] >> abc[2];
+    if (!(f >> compact)) compact = 1;
+    std::cin >> n;
     std::vector<uint32_t> primes(n ? n : 1);
     for (uint32_t i = 0; i < n; i++) std::cin >> primes[i];
     if (!std::cin || K < 1 || K > PFB_SIEVE_MAX_K) return 2;
@@ -50,13 +59,15 @@ int main() {
         });
     // survivor compaction (pfb_sieve_survivors)
     const uint32_t nbits = (uint32_t)K * (uint32_t)K, nwords = (nbits + 31u) / 32u, chunks = (nwords + 31u) / 32u;
-    std::vector<uint32_t> chunk(chunks), out(nbits);
+    std::vector<uint32_t> chunk(chunks), out(compact ? nbits : 1);
     uint32_t total = 0;
-    emu::run_grid(chunks, 1, 32, [&] { surv_count_kernel(mask.data(), nbits, chunk.data()); });
-    emu::run_grid(1, 1, 1024, [&] { surv_scan_kernel(chunk.data(), chunks, &total); });
-    emu::run_grid(chunks, 1, 32, [&] {
-        surv_write_kernel(mask.data(), nbits, K, chunk.data(), out.data(), nbits);
-    });
+    if (compact) {
+        emu::run_grid(chunks, 1, 32, [&] { surv_count_kernel(mask.data(), nbits, chunk.data()); });
+        emu::run_grid(1, 1, 1024, [&] { surv_scan_kernel(chunk.data(), chunks, &total); });
+        emu::run_grid(chunks, 1, 32, [&] {
+            surv_write_kernel(mask.data(), nbits, K, chunk.data(), out.data(), nbits);
+        });
+    }
     char buf[16];
     for (size_t i = 0; i < wpt; i++) {
         snprintf(buf, sizeof buf, "%08x", mask[i]);
