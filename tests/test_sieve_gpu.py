@@ -183,6 +183,26 @@ def test_device_mask_and_survivor_compaction(torch_cuda):
     s.close()
 
 
+def test_k_changes_on_one_caller_stream(torch_cuda):
+    """Asynchronous calls on a caller's stream with K changing between them:
+    a call whose K needs a new split of the prime list first waits for the
+    stream's earlier calls, so every mask equals the oracle's."""
+    torch = torch_cuda
+    P = primes_below(100_000)
+    s = pfb200.Sieve(P)
+    stream = torch.cuda.Stream()
+    abc = (81, 61, 27)
+    Ks = [3000, 100, 3000, 40, 1200]  # small-prime limits 10^4, 4096, 10^4, 4096, 10^4
+    masks = [torch.zeros(pfb200.mask_bytes(K), dtype=torch.uint8, device="cuda") for K in Ks]
+    for K, m in zip(Ks, masks):
+        s.run([abc], K, m, stream=stream.cuda_stream)
+    stream.synchronize()
+    for K, m in zip(Ks, masks):
+        want = oracle.sieve_grid(P, *abc, K)
+        assert (m.cpu().numpy()[:len(want)] == want).all(), K
+    s.close()
+
+
 def test_bad_arguments_rejected(torch_cuda):
     P = primes_below(1000)
     with pytest.raises(pfb200.PfbError):
