@@ -186,6 +186,33 @@ def cpu_sieve_baseline(procs=None, frac=0.05):
                       "one process per core, scaled by prime count" % int(frac * 100)}
 
 
+def e2e_breakdown(pfb200, torch, eng, cands):
+    """The stages of one pfb_mr_test call, timed apart through the batch API
+    (the same calls run_jobs makes): host set-up + uploads + set-up kernel,
+    the main advance by the longest test's steps, the rounds that finish the
+    candidates the round-robin left behind, and the read-back."""
+    t0 = time.perf_counter()
+    b = pfb200.MRBatch(eng, cands, 2)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    b.advance(b.steps_left())
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    done_main = pfb200.batch_steps_done(b)
+    rounds = 0
+    while b.pending() and rounds < 1000:
+        b.advance(4096)
+        rounds += 1
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    done_all = pfb200.batch_steps_done(b)
+    b.results(residues=True)
+    t4 = time.perf_counter()
+    b.close()
+    return {"setup_s": t1 - t0, "main_s": t2 - t1, "topup_s": t3 - t2, "topup_rounds": rounds,
+            "results_s": t4 - t3, "steps_main": done_main, "steps_topup": done_all - done_main}
+
+
 def odd_primes_below(lim):
     """Odd primes <= lim by a plain Eratosthenes in numpy (the sieve's input data)."""
     import numpy as np
@@ -272,6 +299,8 @@ def main():
     ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
     ap.add_argument("--mr-case", choices=sorted(MR_CASES) + ["all"],
                     help="only run a small case of the squaring kernel (8 candidates, 64 squarings; for ncu)")
+    ap.add_argument("--e2e-breakdown", action="store_true",
+                    help="also time the stages of the e2e call apart (one more e2e-sized run)")
     ap.add_argument("--sieve-case", action="store_true",
                     help="only run one K = 9999 sieve triple twice (for ncu)")
     args = ap.parse_args()
@@ -565,6 +594,8 @@ def main():
                "d2h_bytes_per_step": d2h, "candidates": len(sub), "seconds": dt,
                "verdicts": {"probable_prime": int(sum(1 for v in ver if v == 1)), "composite":
                             int(sum(1 for v in ver if v == 0))}}
+        if args.e2e_breakdown:
+            e2e["breakdown"] = e2e_breakdown(pfb200, torch, eng, sub)
 
     if dist is not None:
         dist.barrier()
