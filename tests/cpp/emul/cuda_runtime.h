@@ -48,8 +48,39 @@ inline emu_dim3 gridDim;
 
 namespace emu {
 
+// Context switch: on x86-64 (without a sanitizer, which must see stack
+// switches through swapcontext) a plain switch of the callee-saved registers
+// and the stack pointer; elsewhere ucontext.
+#if defined(__x86_64__) && !defined(__SANITIZE_ADDRESS__)
+#define EMU_FAST_SWITCH 1
+extern "C" void emu_switch(void **save_sp, void *load_sp);
+asm(R"(
+    .text
+    .globl emu_switch
+    .type emu_switch, @function
+emu_switch:
+    pushq %rbp
+    pushq %rbx
+    pushq %r12
+    pushq %r13
+    pushq %r14
+    pushq %r15
+    movq %rsp, (%rdi)
+    movq %rsi, %rsp
+    popq %r15
+    popq %r14
+    popq %r13
+    popq %r12
+    popq %rbx
+    popq %rbp
+    ret
+    .size emu_switch, .-emu_switch
+)");
+#endif
+
 struct Fiber {
     ucontext_t ctx;
+    void *sp = nullptr;  // saved stack pointer (fast switch)
     void *stack = nullptr;
     bool done = false;
 };
@@ -70,13 +101,18 @@ inline std::vector<Group> *groups = nullptr;  // 0: the CTA; 1 + w: warp w
 inline std::vector<unsigned long long> *lane_vals = nullptr;
 inline const std::function<void()> *body = nullptr;
 inline ucontext_t main_ctx;
+inline void *main_sp = nullptr;
 inline int current = 0;
 
 inline void switch_to(int next) {
     const int prev = current;
     current = next;
     threadIdx.x = (unsigned)next;
+#ifdef EMU_FAST_SWITCH
+    emu_switch(&(*fibers)[prev].sp, (*fibers)[next].sp);
+#else
     swapcontext(&(*fibers)[prev].ctx, &(*fibers)[next].ctx);
+#endif
     threadIdx.x = (unsigned)current;
 }
 
@@ -113,8 +149,17 @@ inline void fiber_main(int id) {
     (*body)();
     (*fibers)[id].done = true;
     yield();  // to an unfinished fiber, never back here; none left: to the caller
+#ifdef EMU_FAST_SWITCH
+    void *dead = nullptr;
+    emu_switch(&dead, main_sp);
+#else
     setcontext(&main_ctx);
+#endif
 }
+
+#ifdef EMU_FAST_SWITCH
+inline void fiber_entry() { fiber_main(current); }
+#endif
 
 inline void trampoline(unsigned lo, unsigned hi) {
     (void)hi;
@@ -143,15 +188,29 @@ inline void run_cta(int threads, const std::function<void()> &f) {
     for (int t = 0; t < threads; t++) {
         Fiber &fb = fs[t];
         fb.stack = stacks[t];
+#ifdef EMU_FAST_SWITCH
+        // initial frame: six register slots, then fiber_entry as the return
+        // address, then a null slot so that fiber_entry starts as if called
+        void **p = (void **)(((uintptr_t)fb.stack + stack_bytes) & ~(uintptr_t)15);
+        *--p = nullptr;
+        *--p = (void *)&fiber_entry;
+        for (int r = 0; r < 6; r++) *--p = nullptr;
+        fb.sp = p;
+#else
         getcontext(&fb.ctx);
         fb.ctx.uc_stack.ss_sp = fb.stack;
         fb.ctx.uc_stack.ss_size = stack_bytes;
         fb.ctx.uc_link = &main_ctx;
         makecontext(&fb.ctx, (void (*)())trampoline, 2, (unsigned)t, 0u);
+#endif
     }
     current = 0;
     threadIdx.x = 0;
+#ifdef EMU_FAST_SWITCH
+    emu_switch(&main_sp, fs[0].sp);
+#else
     swapcontext(&main_ctx, &fs[0].ctx);
+#endif
     fibers = nullptr;
     groups = nullptr;
     lane_vals = nullptr;
