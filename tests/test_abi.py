@@ -68,3 +68,26 @@ def test_missing_library_raises_instead_of_falling_back(tmp_path):
             % (os.path.join(ROOT, "prime-finder_b200"), str(tmp_path / "libpfb200.so")))
     out = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=120).stdout
     assert out.startswith("raised") and "is missing" in out
+
+
+def test_headers_serve_c_callers(tmp_path):
+    """The reference's callers are C (worker.c, tests/test_gpu.c): every
+    header in include/*.h compiles as strict C99, and a C program linked
+    against the library runs calls that need no GPU."""
+    import subprocess
+    src = tmp_path / "caller.c"
+    headers = sorted(f for f in os.listdir(INC) if f.endswith(".h"))
+    src.write_text("".join('#include "%s"\n' % h for h in headers) + """
+#include <stdio.h>
+int main(void) {
+    printf("%zu %d\\n", pfb_sieve_mask_bytes(100), trial_div_gpu(NULL, 1, 1, 1, NULL, NULL));
+    return 0;
+}
+""")
+    exe = str(tmp_path / "caller")
+    libdir = os.path.dirname(pfb200.LIB_PATH)
+    cc = subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", INC, str(src), "-o", exe,
+                         "-L", libdir, "-lpfb200", "-Wl,-rpath," + libdir], capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0 and r.stdout.split() == ["1252", "-1"], (r.stdout, r.stderr)
