@@ -91,3 +91,16 @@ int main(void) {
     assert cc.returncode == 0, cc.stderr
     r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
     assert r.returncode == 0 and r.stdout.split() == ["1252", "-1"], (r.stdout, r.stderr)
+
+
+def test_cpp_surface_compiles_and_links(tmp_path):
+    """bench_mr_gpu.cu-style C++ callers of batch_mod_ctx.cuh and
+    miller_rabin_runner.cuh (tests/cpp/mr_api_demo.cpp) compile and link
+    against the library; running them needs a GPU (test_cpp_api_gpu.py)."""
+    import subprocess
+    exe = str(tmp_path / "mr_api_demo")
+    libdir = os.path.dirname(pfb200.LIB_PATH)
+    cc = subprocess.run(["g++", "-O1", "-std=c++17", "-Wall", "-I", INC, "-I", "/usr/local/cuda/include",
+                         os.path.join(ROOT, "tests", "cpp", "mr_api_demo.cpp"), "-o", exe,
+                         "-L", libdir, "-lpfb200", "-Wl,-rpath," + libdir], capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
