@@ -31,3 +31,47 @@ def test_sieve_input_primes():
     P = bench.odd_primes_below(1_000_000)
     assert len(P) == 78497 and P[0] == 3 and P[-1] == 999983  # pi(10^6) = 78498, less the prime 2
     assert len(bench.odd_primes_below(100)) == 24
+
+
+def test_e2e_breakdown_stages_with_a_stand_in_batch():
+    """bench.e2e_breakdown's control flow (the stages of one test call through
+    the batch API) on a stand-in batch object: main advance by the steps left,
+    top-up rounds until nothing is pending, then the read-back."""
+    class Batch:
+        def __init__(self, eng, cands, base):
+            self.left, self.pend, self.done, self.closed = 1000, 3, 0, False
+
+        def steps_left(self):
+            return self.left
+
+        def advance(self, steps):
+            self.done += steps
+            self.left = max(0, self.left - steps)
+            if steps == 4096:
+                self.pend = max(0, self.pend - 1)
+
+        def pending(self):
+            return self.pend
+
+        def results(self, residues=False):
+            return [0], [0]
+
+        def close(self):
+            self.closed = True
+
+    class Fake:
+        MRBatch = Batch
+
+        @staticmethod
+        def batch_steps_done(b):
+            return b.done
+
+    class Torch:
+        class cuda:
+            @staticmethod
+            def synchronize():
+                pass
+
+    out = bench.e2e_breakdown(Fake, Torch, None, [1, 2])
+    assert out["topup_rounds"] == 3 and out["steps_main"] == 1000 and out["steps_topup"] == 3 * 4096
+    assert all(out[k] >= 0 for k in ("setup_s", "main_s", "topup_s", "results_s"))
