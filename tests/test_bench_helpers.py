@@ -75,3 +75,22 @@ def test_e2e_breakdown_stages_with_a_stand_in_batch():
     out = bench.e2e_breakdown(Fake, Torch, None, [1, 2])
     assert out["topup_rounds"] == 3 and out["steps_main"] == 1000 and out["steps_topup"] == 3 * 4096
     assert all(out[k] >= 0 for k in ("setup_s", "main_s", "topup_s", "results_s"))
+
+
+def test_reference_arm_line():
+    """bench.py --impl reference (the reference's CPU path, timed on the host
+    cores) prints one JSON line with the contract's keys; under a launcher,
+    ranks other than 0 print nothing and exit 0."""
+    import json
+    import os
+    import subprocess
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference", "--steps", "1", "--warmup", "0"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads(r.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["metric"] == bench.METRIC and line["unit"] == "tests/s"
+    assert line["value"] > 0 and line["e2e"]["value"] == line["value"] and line["higher_is_better"] is True
+    assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["cores"] >= 1
+    env = dict(os.environ, RANK="1", WORLD_SIZE="2", LOCAL_RANK="1")
+    r1 = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT, env=env)
+    assert r1.returncode == 0 and r1.stdout.strip() == ""
