@@ -65,3 +65,21 @@ def test_strong_lucas_verdicts(emul):
     ns += [rng.getrandbits(b) | 1 | (1 << (b - 1)) for b in (30, 50, 70)]
     out = emul(["2 2 %x" % n for n in ns])
     assert [int(v) for v in out] == [lucas.strong_lucas(n) for n in ns]
+
+
+def _with_d(rng, D, bits, want_prime):
+    while True:
+        n = rng.getrandbits(bits) | (1 << (bits - 1)) | 1
+        if want_prime:
+            n = oracle.nextprime(n)
+        if lucas.selfridge_d(n) == D:
+            return n
+
+
+@pytest.mark.parametrize("D", [5, -7, -11, 13, -15, 17, -19, -23])
+def test_strong_lucas_each_selfridge_class(emul, D):
+    """One composite and one prime per Selfridge class D (Q = (1 - D) / 4:
+    -1, 2, 3, -3, 4, -4, 5, 6), through the emulated Lucas ladder."""
+    rng = random.Random(2000 + D)
+    ns = [_with_d(rng, D, 90, False), _with_d(rng, D, 120, True)]
+    assert [int(v) for v in emul(["2 2 %x" % n for n in ns])] == [lucas.strong_lucas(n) for n in ns]
