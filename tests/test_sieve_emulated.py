@@ -107,3 +107,12 @@ def test_emulated_sieve_in_bounds(tmp_path):
         got, count, surv, err = _run(exe, P5, a, b, c, K, env=env)
         assert "ERROR: AddressSanitizer" not in err
         _check(got, count, surv, P5, a, b, c, K)
+
+
+def test_emulated_sieve_ignores_two_and_non_primes(emul):
+    """The prime list may hold 2 (never a divisor of the odd N and rev(N)),
+    and entries below 2 are ignored: the mask is the one of the odd primes."""
+    P = [p for p in primes_below(20_000).tolist() if p > 2]
+    base = _run(emul, P, 50000, 30000, 100, 100)
+    for extra in ([2] + P, [2, 2] + P[:5] + [1, 0] + P[5:]):
+        assert _run(emul, extra, 50000, 30000, 100, 100)[:3] == base[:3]
