@@ -102,17 +102,23 @@ int trial_div_gpu_grid(const uint32_t *primes, uint32_t n_primes,
  * the reference: it exists for callers that cannot call cudaMalloc (a process
  * whose device memory is reserved up front by another allocator, or a loop
  * that cannot take the device-wide synchronisation cudaFree implies).
- *   d_primes  device array of n_primes odd primes (no repeated entries)
+ *   d_primes  device array of n_primes odd primes
  *   d_mask    device mask block of pfb_sieve_mask_bytes(K) bytes, written
  *             (or OR-ed with PFB_SIEVE_OR) asynchronously on `stream`
  * Limits: one triple per call, 1 <= K <= 9999 (PFB_E_CAPACITY otherwise).
- * Working memory is one fixed 1.16 MB __device__ array inside the library,
- * held by every GPU that loads it until the process exits; nothing is
- * allocated.  All calls share that array: calls that overlap on the GPU (two
- * streams, two host threads) race and must be serialised by the caller.  The
- * first call on a device also looks up the array's device address and sets
- * the tile kernel's shared-memory limit; make that first call before any
- * stream capture.
+ * Working memory is one fixed __device__ array of 1 081 976 bytes (1.08 MB)
+ * inside the library, held by every GPU that loads it until the process
+ * exits; nothing is allocated.  All calls share that array: calls that
+ * overlap on the GPU (two streams, two host threads) race and must be
+ * serialised by the caller.  The first call on a device looks up the array's
+ * device address and sets the tile kernel's shared-memory limit, and keeps
+ * both for the life of the process; make that first call before any stream
+ * capture, and do not call this entry point on a device again after
+ * cudaDeviceReset on it (the kept address belongs to the old context).
+ * Unlike pfb_sieve_run, which rejects a list repeating small primes
+ * (PFB_E_ARG), this call lists each small value once, so a list with repeats
+ * gives the mask of the list without them; even values below 10 000 are
+ * skipped (2 never divides the odd N and rev(N)).
  */
 int pfb_sieve_run_noalloc(const uint32_t *d_primes, uint32_t n_primes, long long a, long long b,
                           long long c, int K, uint32_t *d_mask, unsigned flags, void *stream);

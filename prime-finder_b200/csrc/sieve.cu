@@ -482,26 +482,34 @@ void trial_div_launch(const uint32_t *d_primes, uint32_t n_primes, uint64_t a, u
 
 namespace {
 
-constexpr uint32_t kNoAllocListCap = 10000u / 2u + 2u;  // small primes (< 10000) per list
+constexpr uint32_t kNoAllocLimit = 10000u;                   // small_limit(K) for every K <= 9999
+constexpr uint32_t kNoAllocListCap = kNoAllocLimit / 2u + 2u;  // odd values below the limit, + 2
+constexpr uint32_t kNoAllocSeenWords = kNoAllocLimit / 32u + 1u;
 
 struct NoAllocScratch {
     uint32_t counts[2];
     uint32_t pad0[62];
     long long abc[4];
+    uint32_t seen[kNoAllocSeenWords];  // small values already listed (bit v)
     uint32_t tiny[kNoAllocListCap];
     uint32_t small[kNoAllocListCap];
     SmallRec rec[2 * kNoAllocListCap];
 };
 
-// 1.16 MB: the scratch of one triple at any K <= 9999.
+// 1 081 976 bytes (1.08 MB): the scratch of one triple at any K <= 9999.
+static_assert(sizeof(NoAllocScratch) == 1081976, "the size the header states");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
+// One block: clears the counts and the seen-bitmap, stores the triple.
 __global__ void noalloc_begin_kernel(NoAllocScratch *sc, long long a, long long b, long long c) {
-    sc->counts[0] = 0u;
-    sc->counts[1] = 0u;
-    sc->abc[0] = a;
-    sc->abc[1] = b;
-    sc->abc[2] = c;
+    for (uint32_t w = threadIdx.x; w < kNoAllocSeenWords; w += blockDim.x) sc->seen[w] = 0u;
+    if (threadIdx.x == 0) {
+        sc->counts[0] = 0u;
+        sc->counts[1] = 0u;
+        sc->abc[0] = a;
+        sc->abc[1] = b;
+        sc->abc[2] = c;
+    }
 }
 
 std::mutex g_noalloc_mu;
@@ -553,13 +561,14 @@ extern "C" int pfb_sieve_run_noalloc(const uint32_t *d_primes, uint32_t n_primes
     cudaStream_t st = (cudaStream_t)stream;
     const size_t wpt = pfb_sieve_mask_bytes(K) / 4;
     if (!(flags & PFB_SIEVE_OR)) PFB_CUDA(cudaMemsetAsync(d_mask, 0, wpt * 4, st));
-    noalloc_begin_kernel<<<1, 1, 0, st>>>(sc, a, b, c);
+    noalloc_begin_kernel<<<1, 320, 0, st>>>(sc, a, b, c);
     PFB_CUDA(cudaGetLastError());
     const uint32_t lim = small_limit(K);
     const uint32_t cap = kNoAllocListCap;
     if (n_primes) {
         const int blocks = (int)std::min<uint32_t>((n_primes + 255u) / 256u, (uint32_t)sms * 16u);
-        split_kernel<<<blocks, 256, 0, st>>>(d_primes, n_primes, lim, cap, sc->tiny, sc->small, sc->counts);
+        split_unique_kernel<<<blocks, 256, 0, st>>>(d_primes, n_primes, lim, sc->seen, sc->tiny, sc->small,
+                                                    sc->counts);
         PFB_CUDA(cudaGetLastError());
         // record stride 2*cap: tiny then small; the kernels read the counts on the device
         dim3 g1((2u * cap + 127u) / 128u, 1u);

@@ -303,6 +303,24 @@ __global__ void split_kernel(const uint32_t *__restrict__ primes, uint32_t n, ui
     }
 }
 
+// split_kernel for lists of fixed capacity (the allocation-free entry
+// point): a value is listed once however often the prime list repeats it
+// (seen: a bitmap over [0, s_limit), cleared by the caller), and even values,
+// never prime above 2 (2 eliminates nothing: N and rev(N) are odd), are
+// skipped.  At most the odd values in [3, s_limit) are listed, so lists of
+// s_limit/2 + 2 entries cannot overflow, whatever the input.
+__global__ void split_unique_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
+                                    uint32_t *seen, uint32_t *tiny, uint32_t *small, uint32_t *counts) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = primes[i];
+        if (p < 3u || p >= s_limit || !(p & 1u)) continue;
+        const uint32_t bit = 1u << (p & 31u);
+        if (atomicOr(&seen[p >> 5], bit) & bit) continue;
+        if (p < kTinyLimit) tiny[atomicAdd(&counts[0], 1u)] = p;
+        else small[atomicAdd(&counts[1], 1u)] = p;
+    }
+}
+
 // Set-up of the small-prime records for every triple: rec[t * cap + i];
 // cap = 2 * capacity of each list.
 __global__ void small_setup_kernel(const uint32_t *__restrict__ tiny, const uint32_t *__restrict__ small,

@@ -3,7 +3,9 @@
 // launches are those pfb_sieve_run and pfb_sieve_survivors make for one
 // triple (sieve.cu: ensure_split, enqueue_sieve, pfb_sieve_survivors).
 //
-// Input: "K a b c [compact]", then "n p_1 ... p_n" (the prime list).
+// Input: "K a b c [compact [unique]]", then "n p_1 ... p_n" (the prime list).
+// unique = 1 splits the list as pfb_sieve_run_noalloc does (split_unique_kernel:
+// repeated entries listed once, into lists of fixed capacity).
 // Output: the mask as hexadecimal little-endian words (one line), then the
 // number of survivors and the 64-bit FNV-1a hash of the survivor list
 // (k<<16|j as little-endian uint32), in decimal (one line; "0 0" when
@@ -23,9 +25,10 @@ int main() {
     std::string first;
     std::getline(std::cin, first);
     std::istringstream f(first);
-    int compact = 1;
+    int compact = 1, unique = 0;
     f >> K >> abc[0] >> abc[1] >> abc[2];
     if (!(f >> compact)) compact = 1;
+    if (!(f >> unique)) unique = 0;
     std::cin >> n;
     std::vector<uint32_t> primes(n ? n : 1);
     for (uint32_t i = 0; i < n; i++) std::cin >> primes[i];
@@ -36,7 +39,12 @@ int main() {
     // split of the prime list (ensure_split): a grid-stride kernel, any grid
     const uint32_t lim = small_limit(K), cap = lim / 2u + 2u;
     std::vector<uint32_t> tiny(cap), small(cap), counts(2, 0u);
-    if (n)
+    std::vector<uint32_t> seen(lim / 32u + 1u, 0u);
+    if (n && unique)
+        emu::run_grid(4, 1, 256, [&] {
+            split_unique_kernel(primes.data(), n, lim, seen.data(), tiny.data(), small.data(), counts.data());
+        });
+    else if (n)
         emu::run_grid(4, 1, 256, [&] { split_kernel(primes.data(), n, lim, cap, tiny.data(), small.data(), counts.data()); });
     if (counts[0] > cap || counts[1] > cap) return 3;
     const uint32_t n_small_all = counts[0] + counts[1];

@@ -15,10 +15,14 @@ oracle/mr_oracle.c), the base-2 strong-test residue r = 2^d mod N
   mr_uneven_first32.json  (uneven) the first 32 of the 512 uneven-batch
                           tuples (pfb200.workloads.uneven_tuples: 50 000 -
                           100 000 digits)
+  mr_uneven_first128.json (uneven128) the first 128 of those tuples (12 of
+                          them at most 54 250 digits, the shorter transform
+                          length); records already in mr_uneven_first32.json
+                          are reused, not recomputed
 
 Each 50 000-digit powm takes minutes of one core; the script runs a process
 pool (spawn) over all cores.  Usage:
-  python tests/golden/make_mr_golden.py first16|survivors|uneven
+  python tests/golden/make_mr_golden.py first16|survivors|uneven|uneven128 [processes]
 """
 import hashlib
 import json
@@ -57,14 +61,26 @@ def main():
     if which == "first16":
         pairs = pairs[:16]
     jobs = [(a, b, c, k, j, rev) for (k, j) in pairs for rev in (False, True)]
-    if which == "uneven":
+    known = {}
+    if which in ("uneven", "uneven128"):
         from pfb200.workloads import uneven_tuples
-        jobs = uneven_tuples(512)[:32]
+        jobs = uneven_tuples(512)[:32 if which == "uneven" else 128]
+        old = os.path.join(HERE, "mr_uneven_first32.json")
+        if which == "uneven128" and os.path.exists(old):
+            for r in json.load(open(old))["records"]:
+                known[(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"]))] = r
+    todo = [t for t in jobs if t not in known]
+    procs = int(sys.argv[2]) if len(sys.argv) > 2 else os.cpu_count()
+    # longest first, so the pool's tail is short
+    todo.sort(key=lambda t: -t[0])
     ctx = mp.get_context("spawn")
-    with ctx.Pool(os.cpu_count()) as pool:
-        recs = pool.map(residue_record, jobs, chunksize=1)
+    with ctx.Pool(procs) as pool:
+        for r in pool.imap_unordered(residue_record, todo, chunksize=1):
+            known[(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"]))] = r
+            print("done", len(known), "of", len(jobs), r["a"], r["secs"], flush=True)
+    recs = [known[t] for t in jobs]
     out = {"source": "GMP 6.3 mpz_powm via oracle/mr_oracle.c", "base": 2, "records": recs}
-    if which != "uneven":
+    if which not in ("uneven", "uneven128"):
         out["abc"] = [a, b, c]
     if which == "first16":
         sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -72,7 +88,8 @@ def main():
         if oracle.ref_available():
             out["ref_miller_rabin_test"] = {"%d,%d" % p: oracle.ref_miller_rabin_test(a, b, c, *p)
                                             for p in pairs}
-    names = {"first16": "mr_50k_first16.json", "survivors": "mr_50k_survivors.json", "uneven": "mr_uneven_first32.json"}
+    names = {"first16": "mr_50k_first16.json", "survivors": "mr_50k_survivors.json", "uneven": "mr_uneven_first32.json",
+             "uneven128": "mr_uneven_first128.json"}
     with open(os.path.join(HERE, names[which]), "w") as f:
         json.dump(out, f, indent=1)
     print("wrote", len(recs), "records")

@@ -42,8 +42,8 @@ def emul(tmp_path_factory):
     return exe
 
 
-def _run(exe, P, a, b, c, K, env=None, compact=True):
-    inp = "%d %d %d %d %d\n%d %s\n" % (K, a, b, c, int(compact), len(P), " ".join(map(str, P)))
+def _run(exe, P, a, b, c, K, env=None, compact=True, unique=False):
+    inp = "%d %d %d %d %d %d\n%d %s\n" % (K, a, b, c, int(compact), int(unique), len(P), " ".join(map(str, P)))
     r = subprocess.run([exe], input=inp, capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     first, second = r.stdout.split("\n")[:2]
@@ -116,3 +116,26 @@ def test_emulated_sieve_ignores_two_and_non_primes(emul):
     base = _run(emul, P, 50000, 30000, 100, 100)
     for extra in ([2] + P, [2, 2] + P[:5] + [1, 0] + P[5:]):
         assert _run(emul, extra, 50000, 30000, 100, 100)[:3] == base[:3]
+
+
+def test_emulated_unique_split_tolerates_repeats(tmp_path):
+    """The allocation-free entry point's split (split_unique_kernel) lists a
+    repeated value once into lists of fixed capacity: a prime list with more
+    repeated small entries than the lists hold gives the mask of the list
+    without repeats, and even entries are skipped.  Under AddressSanitizer,
+    so an overflow of the fixed lists would show."""
+    exe = str(tmp_path / "sieve_emul_asan")
+    cc = _build(exe, asan=True)
+    if cc.returncode != 0 and "asan" in cc.stderr.lower():
+        pytest.skip("no AddressSanitizer runtime")
+    assert cc.returncode == 0, cc.stderr
+    env = dict(os.environ, ASAN_OPTIONS="detect_stack_use_after_return=0:detect_leaks=0")
+    P = [p for p in primes_below(20_000).tolist() if p > 2]
+    small = [p for p in P if p < 4096]
+    noisy = [3] * 6000 + small * 3 + [4, 6, 8, 4096] + P + [11] * 100
+    for K in (100, 400):
+        base = _run(exe, P, 50000, 30000, 100, K, env=env)
+        got = _run(exe, noisy, 50000, 30000, 100, K, env=env, unique=True)
+        assert "ERROR: AddressSanitizer" not in got[3]
+        assert got[:3] == base[:3]
+        _check(*got[:3], P, 50000, 30000, 100, K)

@@ -15,6 +15,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 import pfb200
 from conftest import primes_below
 
@@ -42,7 +43,10 @@ def test_noalloc_matches_regular_entry_point_two_calls(torch):
     run = _noalloc()
     P = primes_below(3_000_000)
     d_primes = torch.from_numpy(P.view(np.int32)).cuda()
-    cases = [((50000, 30000, 100), 9999), ((50001, 1098, 100), 2500)]
+    # K = 9999 then 2500 (same small-prime limit, 10 000), then 700 (limit
+    # 4096): the scratch goes from the longer small-prime lists to shorter
+    # ones, so whatever a call leaves in it must not reach the next one
+    cases = [((50000, 30000, 100), 9999), ((50001, 1098, 100), 2500), ((50002, 2095, 101), 700)]
     ref = pfb200.Sieve(P)
     for (a, b, c), K in cases:
         want = ref.run([(a, b, c)], K)
@@ -52,7 +56,25 @@ def test_noalloc_matches_regular_entry_point_two_calls(torch):
         torch.cuda.synchronize()
         got = d_mask.cpu().numpy()
         assert (got == want).all(), (a, b, c, K)
+        if K <= 2500:  # and against the oracle itself (restated trial_div_cpu)
+            o = oracle.sieve_grid(P, a, b, c, K)
+            assert (got[:len(o)] == o).all(), (a, b, c, K)
     ref.close()
+
+
+def test_noalloc_repeated_entries(torch):
+    """A list that repeats small primes more often than the fixed lists hold
+    gives the mask of the list without repeats (each value is listed once)."""
+    run = _noalloc()
+    P = primes_below(300_000)
+    noisy = np.concatenate([np.full(6000, 3, np.uint32), P[P < 10000], P, np.full(50, 7, np.uint32)])
+    d_primes = torch.from_numpy(noisy.view(np.int32)).cuda()
+    a, b, c, K = 50000, 30000, 100, 1200
+    d_mask = torch.zeros(pfb200.mask_bytes(K), dtype=torch.uint8, device="cuda")
+    assert run(d_primes.data_ptr(), len(noisy), a, b, c, K, d_mask.data_ptr(), 0, None) == 0
+    torch.cuda.synchronize()
+    o = oracle.sieve_grid(P, a, b, c, K)
+    assert (d_mask.cpu().numpy()[:len(o)] == o).all()
 
 
 def test_noalloc_or_in_and_limits(torch):
