@@ -139,6 +139,20 @@ def _gmp_powm_sample(args):
     return dt / E.bit_length(), d.bit_length()
 
 
+def _reference_full_test(abc, kj, q):
+    """One call of the reference's own miller_rabin_test (oracle/_ref, built
+    from miller_rabin.c) on N(a,b,c,k,j), timed on one core."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_available():
+        return
+    t0 = time.perf_counter()
+    code = oracle.ref_miller_rabin_test(abc[0], abc[1], abc[2], kj[0], kj[1])
+    q.put({"full_test_s": time.perf_counter() - t0, "miller_rabin_test": code,
+           "what": "reference miller_rabin_test(%d, %d, %d, %d, %d): GMP mpz_probab_prime_p(N, 5) on a "
+                   "composite 50 000-digit N, one core" % (abc[0], abc[1], abc[2], kj[0], kj[1])})
+
+
 def cpu_mr_baseline(pairs, abc, sample_bits=4096, procs=None):
     """GMP mpz_powm(2, d, N) on every host core at once, each on the top
     `sample_bits` bits of d; scaled to full tests (bits(d) squarings)."""
@@ -159,31 +173,71 @@ def cpu_mr_baseline(pairs, abc, sample_bits=4096, procs=None):
 
 
 def _sieve_ref_sample(args):
-    frac_primes, a, b, c = args
+    stride, a, b, c = args
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     P = oracle.primes_below(100_000_000)
-    sub = P[: int(len(P) * frac_primes)]
+    sub = P[::stride].copy()
     t0 = time.perf_counter()
     oracle.ref_trial_div_cpu(sub, a, b, c)
     return (time.perf_counter() - t0) / len(sub), len(P)
 
 
-def cpu_sieve_baseline(procs=None, frac=0.05):
-    """The reference's own trial_div_cpu (100 x 100 grid) on every core, each on
-    a 5% prefix of the primes, scaled to the whole list: pairs/s."""
+def cpu_sieve_baseline(procs=None, stride_ref=20, stride_k9999=100):
+    """Two CPU sieve baselines, both in pairs/s:
+    value: the restated trial_div_cpu (oracle/sieve_oracle.c, OpenMP over the
+      primes) on the K = 9999 grid of the GPU's workload, on every host core,
+      over every 100th prime below 1e8, scaled by prime count;
+    reference_100x100: the reference's own trial_div_cpu (its fixed 100 x 100
+      grid) on every core, one process per core as the reference's CPU ranks
+      run it, each over every 20th prime, scaled by prime count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
-    if not oracle.ref_available():
-        return None
     procs = procs or os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(procs) as pool:
-        res = pool.map(_sieve_ref_sample, [(frac, 50000 + i, 30000, 100) for i in range(procs)])
-    per_core = [1e4 / (t_p * n) for t_p, n in res]
-    return {"value": sum(per_core), "unit": "pairs/s", "cores": procs, "kind": "reference",
-            "sample": "reference trial_div_cpu (100x100 grid) on the first %d%% of the primes < 1e8, "
-                      "one process per core, scaled by prime count" % int(frac * 100)}
+    P = oracle.primes_below(100_000_000)
+    sub = P[::stride_k9999].copy()
+    t0 = time.perf_counter()
+    oracle.sieve_grid(sub, 50000, 30000, 100, 9999, threads=procs)
+    t_k = (time.perf_counter() - t0) * len(P) / len(sub)
+    out = {"value": 9999 * 9999 / t_k, "unit": "pairs/s", "cores": procs, "kind": "port",
+           "sample": "restated trial_div_cpu (oracle/sieve_oracle.c) on the K = 9999 grid of (50000, 30000, "
+                     "100), every %d-th prime < 1e8 on %d threads (%.1f s wall), scaled by prime count"
+                     % (stride_k9999, procs, t_k * len(sub) / len(P))}
+    if oracle.ref_available():
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(procs) as pool:
+            res = pool.map(_sieve_ref_sample, [(stride_ref, 50000 + i, 30000, 100) for i in range(procs)])
+        per_core = [1e4 / (t_p * n) for t_p, n in res]
+        out["reference_100x100"] = {
+            "value": sum(per_core), "unit": "pairs/s", "cores": procs, "kind": "reference",
+            "sample": "reference trial_div_cpu (its 100x100 grid) over every %d-th prime < 1e8, one process "
+                      "per core, scaled by prime count" % stride_ref}
+    return out
+
+
+def reference_gpu_sieve(primes, abc, ours_words):
+    """The reference's own trial_div_gpu (trial_div.cu, built unmodified for
+    sm_100a into oracle/_ref) on the same triple and prime list as the
+    drop-in: one untimed call, then two timed by its own gpu_timing_t; its 313
+    words must equal the drop-in's."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    if not oracle.ref_gpu_available():
+        return None
+    bits, rc, _ = oracle.ref_trial_div_gpu(primes, *abc)
+    if rc != 0:
+        return {"error": "trial_div_gpu returned %d" % rc}
+    calls = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        bits, rc, tm = oracle.ref_trial_div_gpu(primes, *abc)
+        tm["call_s"] = time.perf_counter() - t0
+        calls.append(tm)
+    return {"kind": "reference", "build": "reference trial_div.cu, nvcc -O3 --use_fast_math, sm_100a",
+            "call_s": statistics.mean(c["call_s"] for c in calls),
+            "kernel_s": statistics.mean(c["kernel"] for c in calls),
+            "upload_s": statistics.mean(c["upload"] for c in calls),
+            "same_words": bool((bits == ours_words).all())}
 
 
 def e2e_breakdown(pfb200, torch, eng, cands):
@@ -289,13 +343,18 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--chunk", type=int, default=1024, help="squarings per candidate per step")
-    ap.add_argument("--e2e-batch", type=int, default=0, help="candidates in the e2e call (0 = one per SM)")
+    ap.add_argument("--e2e-batch", type=int, default=0, help="candidates in the e2e call (0 = the whole batch)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-calibration", action="store_true",
+                    help="reference arm: skip the full-length miller_rabin_test timed beside the samples")
     ap.add_argument("--no-uneven", action="store_true", help="skip the 512-candidate uneven batch")
     ap.add_argument("--sieve-triples", type=int, default=4)
-    ap.add_argument("--serve-secs", type=float, default=0.0,
-                    help="also run the serving loop (Poisson arrivals of 50k-100k-digit requests) this long")
+    ap.add_argument("--serve-secs", type=float, default=None,
+                    help="seconds of Poisson arrivals of 50k-100k-digit requests for the serving leg, which "
+                         "then drains (default 180 on one GPU, 0 = no serving leg; off under torchrun)")
+    ap.add_argument("--serve-drain", type=float, default=480.0,
+                    help="longest wait for the requests in flight once arrivals stop")
     ap.add_argument("--serve-load", type=float, default=1.2, help="arrival rate / measured capacity")
     ap.add_argument("--mr-case", choices=sorted(MR_CASES) + ["all"],
                     help="only run a small case of the squaring kernel (8 candidates, 64 squarings; for ncu)")
@@ -321,12 +380,33 @@ def main():
         import json as _j
         g = _j.load(open(os.path.join(ROOT, "tests", "golden", "sieve_50000_30000_100.json")))
         pairs = [tuple(x) for x in g["survivors_99"]]
+        batch_pairs = uniform_batch_pairs(pairs)
+        cores = os.cpu_count() or 1
+        # calibration: the reference's own miller_rabin_test (GMP BPSW on N; N is
+        # composite, so one full 50 000-digit base-2 powm) on one core, beside the samples
+        ctx = mp.get_context("spawn")
+        cal_q = ctx.Queue()
+        cal = ctx.Process(target=_reference_full_test, args=(abc1, batch_pairs[0], cal_q))
+        if not args.no_calibration:
+            cal.start()
         t0 = time.perf_counter()
         steps = []
         for _ in range(args.warmup + args.steps):
-            steps.append(cpu_mr_baseline(uniform_batch_pairs(pairs), abc1, sample_bits=1024))
-        vals = [s["value"] for s in steps[args.warmup:]]
-        v = statistics.mean(vals)
+            steps.append(cpu_mr_baseline(batch_pairs, abc1, sample_bits=1024, procs=max(1, cores - 1)))
+        per_core = statistics.mean(s["per_core"] for s in steps[args.warmup:])
+        v = per_core * cores
+        calib = None
+        if not args.no_calibration:
+            try:
+                calib = cal_q.get(timeout=900)
+                est = 1.0 / statistics.mean(s["per_core"] for s in steps)
+                calib["sampled_estimate_s"] = est
+                calib["estimate_over_full"] = est / calib["full_test_s"]
+            except Exception:
+                pass
+            cal.join(timeout=10)
+            if cal.is_alive():
+                cal.terminate()
         last = steps[-1]
         print(json.dumps({
             "impl": "reference", "metric": METRIC,
@@ -334,8 +414,9 @@ def main():
             "ms_per_step": 1e3 * (time.perf_counter() - t0) / max(1, len(steps)), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "candidates": 256, "parallelism": "replicas"},
-            "cpu_baseline": {"kind": last["kind"], "cores": last["cores"], "sample": last["sample"], "value": v,
-                             "unit": "tests/s"},
+            "cpu_baseline": {"kind": last["kind"], "cores": cores,
+                             "sample": last["sample"] + "; per-core rate x %d cores" % cores, "value": v,
+                             "unit": "tests/s", "calibration": calib},
             "e2e": {"value": v, "unit": "tests/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
 
@@ -419,11 +500,12 @@ def main():
     p0.close()
     del d_p0
     t = pfb200.GpuTiming()
-    pfb200.trial_div_gpu(primes, *abc1, None, t)
+    dropin_words = pfb200.trial_div_gpu(primes, *abc1, None, t)
     t0 = time.perf_counter()
     for _ in range(3):
         pfb200.trial_div_gpu(primes, *abc1, None, t)
     dropin_s = (time.perf_counter() - t0) / 3
+    ref_gpu_sieve = reference_gpu_sieve(primes, abc1, dropin_words) if rank == 0 and not args.no_cpu else None
 
     # --- Miller-Rabin: resident batch ---------------------------------------
     pairs = uniform_batch_pairs(survivors, seed=replicas.rank_seed(1, rank))  # each rank its own batch
@@ -466,21 +548,15 @@ def main():
     ms_per_step = 1e3 * t_mr / args.steps
     batch.close()
 
-    # plain form: one candidate per call
-    one = pfb200.MRBatch(eng, cands[:1], 2)
-    with torch.cuda.stream(stream):
-        one.advance(256, stream.cuda_stream)
-        stream.synchronize()
-        d0 = pfb200.batch_steps_done(one)
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        one.advance(1024, stream.cuda_stream)
-        e1.record(stream)
-        stream.synchronize()
-        d1 = pfb200.batch_steps_done(one)
-    plain_sq_s = (d1 - d0) / (e0.elapsed_time(e1) / 1e3)
-    plain_tests_s = plain_sq_s / sq_per_test
-    one.close()
+    # plain form: one candidate per call, through the C ABI call a drop-in
+    # caller makes (pfb_mr_test on one number: host set-up, upload, the whole
+    # test, read-back)
+    barrier()
+    t0 = time.perf_counter()
+    pv, _ = eng.test(cands[:1], 2, residues=True)
+    torch.cuda.synchronize()
+    plain_s = max_over_ranks(time.perf_counter() - t0)
+    plain_tests_s = 1.0 / plain_s
 
     # uneven batch: 512 candidates of 50 000 - 100 000 digits resident at once,
     # every length advanced by the same persistent launches
@@ -528,7 +604,8 @@ def main():
 
     # --- serving: continuous batching under Poisson arrivals ---------------
     serving = None
-    if args.serve_secs > 0:
+    serve_secs = args.serve_secs if args.serve_secs is not None else (180.0 if world == 1 else 0.0)
+    if serve_secs > 0:
         import random
         rng = random.Random(3)
         # requests: N and rev(N) as separate requests, a ~ U[50000, 100000], c ~ U[100, 1000],
@@ -536,9 +613,12 @@ def main():
         def draw():
             return pfb200.build_candidate(*serving_draw(rng))
         props = torch.cuda.get_device_properties(dev)
-        resident = 2 * props.multi_processor_count
-        # served capacity on this request mix: a resident batch of `resident` draws,
-        # squarings/s over its mean exponent length
+        # one resident request per SM: a request's squarings then run on an SM
+        # of their own (time-to-verdict = its sequential squaring time), and the
+        # device's throughput is that of two per SM (the autotuner's columns)
+        resident = props.multi_processor_count
+        # served capacity on this request mix: a resident batch of `resident`
+        # draws, squarings/s over its mean exponent length
         mix = [draw() for _ in range(resident)]
         mb = pfb200.MRBatch(eng, mix, 2)
         with torch.cuda.stream(stream):
@@ -556,24 +636,34 @@ def main():
         rate = args.serve_load * cap_tests_s
         srv = pfb200.MRServer(eng, max_resident=resident, hbm_budget_bytes=150 * 10**9, chunk_steps=256)
         t_start = time.perf_counter()
-        next_t, tag, lat, pending = 0.0, 0, [], 0
-        while time.perf_counter() - t_start < args.serve_secs:
-            now = time.perf_counter() - t_start
-            while next_t <= now:
-                srv.submit(draw(), tag)
-                tag += 1
-                next_t += rng.expovariate(rate)
-            for r in srv.poll(256, 50):
-                lat.append(r["done_s"] - r["submit_s"])
+        next_t, tag, lat, done_in_window = 0.0, 0, [], 0
+        with ClockSampler(dev) as serve_clocks:
+            while time.perf_counter() - t_start < serve_secs:
+                now = time.perf_counter() - t_start
+                while next_t <= now:
+                    srv.submit(draw(), tag)
+                    tag += 1
+                    next_t += rng.expovariate(rate)
+                for r in srv.poll(256, 50):
+                    lat.append(r["done_s"] - r["submit_s"])
+            done_in_window = len(lat)
+            t_drain = time.perf_counter()
+            while len(lat) < tag and time.perf_counter() - t_drain < args.serve_drain:
+                for r in srv.poll(256, 200):
+                    lat.append(r["done_s"] - r["submit_s"])
+        drain_s = time.perf_counter() - t_drain
         st = srv.stats()
         srv.close()
         lat.sort()
         pct = (lambda q: lat[min(len(lat) - 1, int(q * len(lat)))] if lat else None)
-        serving = {"seconds": args.serve_secs, "arrival_rate_per_s": rate, "submitted": tag,
-                   "completed": len(lat), "tests_per_s": len(lat) / args.serve_secs,
-                   "p50_s": pct(0.50), "p99_s": pct(0.99), "resident_at_end": st["resident"],
-                   "queued_at_end": st["queued"], "launches": st["launches"],
-                   "capacity_tests_per_s": cap_tests_s, "max_resident": resident, "hbm_budget_bytes": 150 * 10**9,
+        serving = {"arrival_seconds": serve_secs, "drain_seconds": drain_s, "arrival_rate_per_s": rate,
+                   "submitted": tag, "completed": len(lat), "tests_per_s": done_in_window / serve_secs,
+                   "p50_s": pct(0.50), "p99_s": pct(0.99), "max_s": lat[-1] if lat else None,
+                   "resident_at_end": st["resident"], "queued_at_end": st["queued"], "launches": st["launches"],
+                   "capacity_tests_per_s": cap_tests_s, "max_resident": resident,
+                   "hbm_budget_bytes": 150 * 10**9, "clocks": serve_clocks.summary(),
+                   "latency_over": "every request submitted in the arrival window (arrival to verdict), "
+                                   "after the drain; tests_per_s counts verdicts inside the window",
                    "workload": "Poisson arrivals (seed 3) of N / rev(N), a ~ U[50000,100000], "
                                "k,j ~ U[1,9999], at %.2fx the estimated capacity" % args.serve_load}
 
@@ -581,7 +671,7 @@ def main():
     e2e = None
     if not args.no_e2e:
         props = torch.cuda.get_device_properties(dev)
-        nb = args.e2e_batch or props.multi_processor_count
+        nb = args.e2e_batch or len(cands)
         sub = cands[:nb]
         barrier()
         t0 = time.perf_counter()
@@ -609,7 +699,8 @@ def main():
         "dtype": "u32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "candidates": n, "squarings_per_step": chunk, "squarings_per_test": sq_per_test,
                    "l2": "flushed between timed steps (256 MiB write)", "parallelism": "replicas"},
-        "plain": {"value": plain_tests_s, "unit": "tests/s", "form": "one candidate per call"},
+        "plain": {"value": plain_tests_s, "unit": "tests/s", "seconds": plain_s,
+                  "form": "one candidate per call: pfb_mr_test on one 50 000-digit number from host limbs"},
         "served_over_plain": tests_s / world / plain_tests_s,
         "uneven": uneven,
         "autotune": autotune,
@@ -618,7 +709,8 @@ def main():
                   "ms_per_triple": 1e3 / (sieve_pairs_s / world / (K * K)),
                   "hbm_compulsory_gbs": sieve_gbs, "hbm_compulsory_bytes_per_triple": sieve_bytes,
                   "dropin_100x100_s": dropin_s, "dropin_timing": {"upload": t.upload, "kernel": t.kernel,
-                                                                  "download": t.download}},
+                                                                  "download": t.download},
+                  "reference_gpu_100x100": ref_gpu_sieve},
         "roofline": roofline,
         "cpu_baseline": cpu,
         "cpu_baseline_sieve": cpu_sieve,

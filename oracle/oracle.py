@@ -11,6 +11,9 @@ Two families of libraries are loaded:
   - the reference's own ``trial_div_cpu.c``, ``prime_list.c``,
   ``miller_rabin.c``, ``sieve_table.c`` and ``sieve.c``, compiled unmodified
   by ``oracle/Makefile``.
+* ``_ref/libref_trial_div_gpu.so`` - the reference's own GPU sieve
+  (``trial_div.cu``), compiled unmodified for sm_100a: the baseline kernel the
+  drop-in ``trial_div_gpu`` is timed against.
 """
 from __future__ import annotations
 
@@ -132,6 +135,37 @@ def ref_trial_div_cpu(primes: np.ndarray, a: int, b: int, c: int,
     pl = _PrimeList(_ptr(primes, C.c_uint32), len(primes))
     _ref_sieve.trial_div_cpu(C.byref(pl), a, b, c, _ptr(bits, C.c_uint32))
     return bits
+
+
+class _GpuTiming(C.Structure):
+    # trial_div.h: { double upload, kernel, download; }
+    _fields_ = [("upload", C.c_double), ("kernel", C.c_double), ("download", C.c_double)]
+
+
+_ref_gpu = None
+
+
+def ref_gpu_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libref_trial_div_gpu.so"))
+
+
+def ref_trial_div_gpu(primes: np.ndarray, a: int, b: int, c: int,
+                      bits: Optional[np.ndarray] = None):
+    """The reference's own trial_div_gpu (trial_div.cu:155-224) on the current
+    CUDA device: returns (313 u32 words, rc, {upload, kernel, download} s)."""
+    global _ref_gpu
+    if _ref_gpu is None:
+        _ref_gpu = C.CDLL(os.path.join(REF_DIR, "libref_trial_div_gpu.so"))
+        _ref_gpu.trial_div_gpu.argtypes = [C.POINTER(_PrimeList), C.c_longlong, C.c_longlong,
+                                           C.c_longlong, C.POINTER(C.c_uint32), C.POINTER(_GpuTiming)]
+        _ref_gpu.trial_div_gpu.restype = C.c_int
+    primes = np.ascontiguousarray(primes, dtype=np.uint32)
+    if bits is None:
+        bits = np.zeros(313, dtype=np.uint32)
+    pl = _PrimeList(_ptr(primes, C.c_uint32), len(primes))
+    t = _GpuTiming()
+    rc = _ref_gpu.trial_div_gpu(C.byref(pl), a, b, c, _ptr(bits, C.c_uint32), C.byref(t))
+    return bits, rc, {"upload": t.upload, "kernel": t.kernel, "download": t.download}
 
 
 class _SieveTable(C.Structure):

@@ -217,12 +217,18 @@ def test_uniform_batch_every_candidate_residue(mr):
 
 
 def test_uneven_batch_subset_residues(mr):
-    """The first 32 uneven-batch candidates (50 000 - 100 000 digits, both
-    transform lengths in one batch) against GMP."""
+    """The first 128 of the 512 uneven-batch candidates (50 000 - 100 000
+    digits; 12 of them at the shorter transform length, so both lengths share
+    the batch's launches) against GMP: residues word for word (SHA-256 and
+    low 64 bits), verdicts bit for bit."""
     from pfb200.workloads import uneven_tuples
-    g = _golden("mr_uneven_first32.json")
-    recs = g["records"]
-    assert [(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs] == uneven_tuples(512)[:32]
+    name = "mr_uneven_first128.json"
+    if not os.path.exists(os.path.join(GOLD, name)):
+        name = "mr_uneven_first32.json"
+    recs = _golden(name)["records"]
+    assert [(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"])) for r in recs] == \
+        uneven_tuples(512)[:len(recs)]
+    assert len({r["bits"] > 22 * (1 << 13) - 36 for r in recs}) == 2  # both transform lengths
     _check_records(mr, recs)
 
 

@@ -4,6 +4,9 @@ Candidates of different lengths are streamed into the server while others
 are resident (staggered submission), and each verdict and residue must equal
 the one-candidate-per-call result and GMP's (oracle), word for word.
 """
+import hashlib
+import json
+import os
 import random
 import time
 
@@ -89,3 +92,31 @@ def test_invalid_requests_reported(engine):
     got = _drain(srv, 3, 60)
     srv.close()
     assert got[1]["verdict"] == -1 and got[2]["verdict"] == -1 and got[3]["verdict"] == 1
+
+
+def test_full_size_requests_in_the_mix(engine):
+    """Ten 50 000 - 100 000-digit requests of the uneven workload (both
+    transform lengths: four at <= 54 250 digits) through a server with eight
+    slots: two requests wait for a slot and are admitted while the others run.
+    Every residue must hash to GMP's (tests/golden/mr_uneven_first32.json)."""
+    path = os.path.join(os.path.dirname(__file__), "golden", "mr_uneven_first32.json")
+    recs = json.load(open(path))["records"]
+    pick = [0, 1, 2, 4, 6, 3, 5, 7, 22, 23]   # 3, 5, 22, 23: the shorter transform length
+    assert sum(1 for i in pick if recs[i]["a"] <= 54250) == 4
+    srv = pfb200.MRServer(engine, max_resident=8, chunk_steps=256)
+    Ns = {}
+    for i in pick:
+        r = recs[i]
+        Ns[i] = oracle.build_candidate(r["a"], r["b"], r["c"], r["k"], r["j"], bool(r["rev"]))
+        srv.submit(Ns[i], tag=i, residue=True)
+    got = _drain(srv, len(pick), timeout_s=600)
+    st = srv.stats()
+    srv.close()
+    assert len(got) == len(pick), st
+    assert max(g["admit_s"] for g in got.values()) > min(g["done_s"] for g in got.values())  # admitted mid-run
+    for i in pick:
+        r, N, x = recs[i], Ns[i], got[i]["residue"]
+        n16 = (N.bit_length() + 15) // 16
+        assert "%016x" % (x & (2**64 - 1)) == r["low64"], i
+        assert hashlib.sha256(x.to_bytes(2 * n16, "little")).hexdigest() == r["sha256"], i
+        assert got[i]["verdict"] == r["sprp2"]

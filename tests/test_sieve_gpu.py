@@ -209,3 +209,48 @@ def test_bad_arguments_rejected(torch_cuda):
         pfb200.trial_div_gpu_grid(P, [(10, 5, 1)], 10000)
     with pytest.raises(pfb200.PfbError):
         pfb200.trial_div_gpu_grid(P, [(10, -5, 1)], 100)
+
+
+def test_drop_in_equals_reference_gpu_kernel(torch_cuda, primes_1e8):
+    """The reference's own trial_div_gpu (trial_div.cu, built unmodified for
+    sm_100a) and the drop-in give the same 313 words: the test_gpu.c triples
+    with its primes 3..97 (tests/test_gpu.c:158-177), OR-in on a pre-set
+    mask, and (50000, 30000, 100) with every odd prime below 1e8."""
+    if not oracle.ref_gpu_available():
+        pytest.skip("reference GPU sieve not built (oracle/_ref)")
+    small = primes_below(97)
+    pre = np.zeros(313, dtype=np.uint32)
+    pre[[0, 100, 312]] = [0x1, 0xF0F0F0F0, 0x80]
+    for (a, b, c), P, start in [((15, 8, 3), small, None), ((20, 10, 5), small, None),
+                                ((25, 12, 6), small, pre), ((50000, 30000, 100), primes_1e8, None)]:
+        want, rc, _ = oracle.ref_trial_div_gpu(P, a, b, c, None if start is None else start.copy())
+        assert rc == 0
+        got = pfb200.trial_div_gpu(P, a, b, c, None if start is None else start.copy())
+        assert (got == want).all(), (a, b, c)
+
+
+def test_k9999_full_grid_all_primes_vs_oracle_hashes(torch_cuda, primes_1e8):
+    """The wide-grid workload at full size: K = 9999 (99 980 001 pairs) with
+    every odd prime below 1e8, four triples in one call.  Each mask must hash
+    to the oracle's (restated trial_div_cpu; tests/golden/sieve_k9999_full.json,
+    made by tests/golden/make_sieve_k9999_golden.py), with the same number of
+    survivors and the same first survivors in k-major order."""
+    import hashlib
+    path = os.path.join(GOLD, "sieve_k9999_full.json")
+    if not os.path.exists(path):
+        pytest.skip("sieve_k9999_full.json not generated")
+    g = json.load(open(path))
+    K = g["K"]
+    assert K == 9999 and g["primes"] == len(primes_1e8)
+    abc = [tuple(r["abc"]) for r in g["records"]]
+    s = pfb200.Sieve(primes_1e8)
+    masks = s.run(abc, K)
+    blk, nb = pfb200.mask_bytes(K), g["mask_bytes"]
+    for t, r in enumerate(g["records"]):
+        m = masks[t * blk: t * blk + nb]
+        assert hashlib.sha256(m.tobytes()).hexdigest() == r["sha256"], r["abc"]
+        bits = np.unpackbits(m, bitorder="little")[:K * K]
+        assert K * K - int(bits.sum()) == r["survivors"]
+        idx = np.flatnonzero(bits == 0)[:len(r["first_survivors"])]
+        assert [[int(q // K) + 1, int(q % K) + 1] for q in idx] == r["first_survivors"]
+    s.close()
