@@ -113,6 +113,44 @@ int pfb_mr_batch_results(pfb_mr_batch_t *b, int8_t *verdict, uint16_t *residue, 
 void pfb_mr_batch_destroy(pfb_mr_batch_t *b);
 
 /*
+ * Per-operation modular context: the reference's BatchModCtx methods
+ * (batch_mod_ctx.cuh:132-179, batch_mod_ctx.cu:82-335) as a C ABI, run by
+ * the engine one Montgomery step per call.  Operands use the reference's
+ * layout: n_limbs 16-bit limbs per modulus, one per uint64, little-endian,
+ * n_batch moduli back to back.  The working form ("residue") of x is
+ * x R mod N, fully reduced, with R = 2^(22 H) of the modulus' transform
+ * length H (the reference's Montgomery form with its own R).
+ *   create        host set-up of every modulus (odd, > 1, at most
+ *                 PFB_MR_MAX_BITS bits; PFB_E_ARG otherwise) and transforms
+ *                 of N, N' (synchronous)
+ *   to_residue    host x -> host working form (mod_residue_forward)
+ *   from_residue  device working form -> host x (mod_residue_backward);
+ *                 synchronises
+ *   check_passed  d_passed[b] = (r_b is the working form of 1 or N - 1)
+ *   modsq/modmul  d_out = working form of a^2 / a b, from working forms
+ *   sq_raw/mul_raw  d_out = the full product, n_sum = 2 n_limbs + 16 limbs
+ *                 per modulus (the reference's n_sum), no reduction
+ * Device pointers; each call is asynchronous on `stream` (NULL = the
+ * engine's stream).  A context's scratch is shared by its calls: calls on one
+ * context must not overlap on the GPU.
+ */
+typedef struct pfb_mr_ctx pfb_mr_ctx_t;
+int pfb_mr_ctx_create(pfb_mr_t *e, const uint64_t *N_all, int n_limbs, int n_batch, pfb_mr_ctx_t **out);
+void pfb_mr_ctx_destroy(pfb_mr_ctx_t *c);
+int pfb_mr_ctx_n_sum(const pfb_mr_ctx_t *c);
+/* Device arrays the context owns ([n_batch][n_limbs] 16-bit limbs in uint64):
+ * the moduli, and the working forms of 1 and of N - 1.  Any may be NULL. */
+int pfb_mr_ctx_buffers(const pfb_mr_ctx_t *c, const uint64_t **d_N, const uint64_t **d_one,
+                       const uint64_t **d_nm1);
+int pfb_mr_ctx_to_residue(pfb_mr_ctx_t *c, const uint64_t *x_all, uint64_t *out_all);
+int pfb_mr_ctx_from_residue(pfb_mr_ctx_t *c, const uint64_t *d_x, uint64_t *out_all);
+int pfb_mr_ctx_check_passed(pfb_mr_ctx_t *c, const uint64_t *d_r, uint8_t *d_passed, void *stream);
+int pfb_mr_ctx_modsq(pfb_mr_ctx_t *c, const uint64_t *d_a, uint64_t *d_out, void *stream);
+int pfb_mr_ctx_modmul(pfb_mr_ctx_t *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, void *stream);
+int pfb_mr_ctx_sq_raw(pfb_mr_ctx_t *c, const uint64_t *d_a, uint64_t *d_out, void *stream);
+int pfb_mr_ctx_mul_raw(pfb_mr_ctx_t *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out, void *stream);
+
+/*
  * Serving: continuous batching of strong tests (no counterpart in the
  * reference, which tests one fixed batch per call: bench_mr_gpu.cu:209-256).
  * Requests arrive one by one from any thread; host workers do the set-up;

@@ -19,6 +19,7 @@
 #include "mr_tables_host.h"
 #include "pfb_mr.h"
 
+#include "mr_ctx_kernels.cuh"
 #include "mr_kernels.cuh"
 #include "mr_prep_host.h"
 
@@ -90,6 +91,7 @@ extern "C" int pfb_mr_create(pfb_mr_t **out, int device) {
         const int mx = (int)std::max(smem_bytes(LOG_LCTA), smem_bytes(LOG_LSEQ));
         ce = cudaFuncSetAttribute(persist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         if (ce == cudaSuccess) ce = cudaFuncSetAttribute(prep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+        if (ce == cudaSuccess) ce = cudaFuncSetAttribute(ctx_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
         if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "smem attribute", __FILE__, __LINE__);
     }
     if (rc) {
@@ -1159,4 +1161,233 @@ extern "C" void pfb_mr_server_destroy(pfb_mr_server_t *s) {
     cudaFree(s->d_table_mem);
     cudaStreamDestroy(s->stream);
     delete s;
+}
+
+// ---------------------------------------------------------------------------
+// Per-operation modular context (BatchModCtx's methods).
+
+struct pfb_mr_ctx {
+    pfb_mr *e = nullptr;
+    int n = 0, n16 = 0, maxlog = LOG_LMIN;
+    uint8_t *d_arena = nullptr;
+    JobDev *d_jobs = nullptr;
+    CtxExtra *d_ex = nullptr;
+    uint64_t *d_one = nullptr, *d_nm1 = nullptr, *d_tmp = nullptr, *d_n = nullptr;  // [n][n16] each
+    std::vector<HostPrep> hp;
+};
+
+namespace {
+
+int ctx_fail(pfb_mr_ctx *c, int rc) {
+    if (c) {
+        cudaFree(c->d_arena);
+        delete c;
+    }
+    return rc;
+}
+
+std::vector<uint64_t> widen16(const pfb::big::Words &w, size_t n16) {
+    std::vector<uint16_t> t(n16);
+    pfb::big::to_u16(w, t.data(), n16);
+    return std::vector<uint64_t>(t.begin(), t.end());
+}
+
+int ctx_launch(pfb_mr_ctx *c, const uint64_t *a, const uint64_t *b, uint64_t *out, int out_stride, int op,
+               void *stream) {
+    if (!c || !a || !out || ((op == CTX_MODMUL || op == CTX_RAW_MUL) && !b)) {
+        pfb::set_error("pfb_mr_ctx: bad argument");
+        return PFB_E_ARG;
+    }
+    PFB_CUDA(cudaSetDevice(c->e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->e->stream;
+    ctx_kernel<<<c->n, THREADS, smem_bytes(c->maxlog), st>>>(c->d_jobs, c->d_ex, a, b ? b : a, out, c->n16,
+                                                              out_stride, op, c->e->tw);
+    PFB_CUDA(cudaGetLastError());
+    return PFB_OK;
+}
+
+}  // namespace
+
+extern "C" int pfb_mr_ctx_create(pfb_mr_t *e, const uint64_t *N_all, int n_limbs, int n_batch, pfb_mr_ctx_t **out) {
+    if (!out || !e || !N_all || n_limbs <= 0 || n_batch <= 0) {
+        pfb::set_error("pfb_mr_ctx_create: bad argument");
+        return PFB_E_ARG;
+    }
+    *out = nullptr;
+    PFB_CUDA(cudaSetDevice(e->device));
+    pfb_mr_ctx *c = new pfb_mr_ctx();
+    c->e = e;
+    c->n = n_batch;
+    c->n16 = n_limbs;
+    std::vector<uint16_t> n16((size_t)n_limbs * n_batch);
+    for (size_t i = 0; i < n16.size(); i++) {
+        if (N_all[i] > 0xFFFFu) {
+            pfb::set_error("pfb_mr_ctx_create: limb %zu is not a 16-bit value", i);
+            return ctx_fail(c, PFB_E_ARG);
+        }
+        n16[i] = (uint16_t)N_all[i];
+    }
+    std::vector<pfb_mr_number_t> nums(n_batch);
+    for (int i = 0; i < n_batch; i++) nums[i] = pfb_mr_number_t{n16.data() + (size_t)i * n_limbs, n_limbs};
+    // base 2 sizes R > 64 N: products of two reduced operands stay below 2N after REDC
+    prep_all(nums.data(), n_batch, 2u, 1, nullptr, c->hp);
+    std::vector<Layout> lay(n_batch);
+    size_t words = 0;
+    for (int i = 0; i < n_batch; i++) {
+        if (!c->hp[i].ok) {
+            pfb::set_error("pfb_mr_ctx_create: modulus %d is not odd, > 1 and at most %d bits", i, PFB_MR_MAX_BITS);
+            return ctx_fail(c, PFB_E_ARG);
+        }
+        lay[i] = layout_for(c->hp[i].logl, 1, true);  // the Lucas layout: gy [2][L] and spare H-word buffers
+        words += lay[i].total;
+        c->maxlog = std::max(c->maxlog, c->hp[i].logl);
+    }
+    const size_t job_bytes = ((size_t)n_batch * sizeof(JobDev) + 255) & ~(size_t)255;
+    const size_t ex_bytes = ((size_t)n_batch * sizeof(CtxExtra) + 255) & ~(size_t)255;
+    const size_t v_bytes = (((size_t)n_batch * n_limbs * sizeof(uint64_t)) + 255) & ~(size_t)255;
+    const size_t need = job_bytes + ex_bytes + 4 * v_bytes + words * sizeof(uint32_t);
+    if (cudaMalloc(&c->d_arena, need) != cudaSuccess) {
+        cudaGetLastError();
+        pfb::set_error("pfb_mr_ctx_create: cannot allocate %zu bytes of device memory", need);
+        return ctx_fail(c, PFB_E_NOMEM);
+    }
+    c->d_jobs = (JobDev *)c->d_arena;
+    c->d_ex = (CtxExtra *)(c->d_arena + job_bytes);
+    c->d_one = (uint64_t *)(c->d_arena + job_bytes + ex_bytes);
+    c->d_nm1 = (uint64_t *)(c->d_arena + job_bytes + ex_bytes + v_bytes);
+    c->d_tmp = (uint64_t *)(c->d_arena + job_bytes + ex_bytes + 2 * v_bytes);
+    c->d_n = (uint64_t *)(c->d_arena + job_bytes + ex_bytes + 3 * v_bytes);
+    uint32_t *d_words = (uint32_t *)(c->d_arena + job_bytes + ex_bytes + 4 * v_bytes);
+    std::vector<JobDev> jobs(n_batch);
+    std::vector<CtxExtra> ex(n_batch);
+    std::vector<uint64_t> one((size_t)n_batch * n_limbs), nm1((size_t)n_batch * n_limbs);
+    size_t off = 0;
+    for (int i = 0; i < n_batch; i++) {
+        const HostPrep &h = c->hp[i];
+        const Layout &l = lay[i];
+        uint32_t *w = d_words + off;
+        JobDev &j = jobs[i];
+        memset(&j, 0, sizeof(j));
+        j.nph = w + l.nph;
+        j.nh = w + l.nh;
+        j.npl = w + l.npl;
+        j.nl = w + l.nl;
+        j.x = w + l.x;
+        j.res = w + l.res;
+        if (h.logl > LOG_LCTA) {
+            j.spill_s = w + l.ss;
+            j.spill_t = w + l.st;
+            j.ybuf = w + l.yb;
+        }
+        j.logl = h.logl;
+        j.phase = 0;
+        ex[i].gy = w + l.gy;
+        ex[i].yl = w + l.lt;
+        const size_t H = h.nl.size();
+        PFB_CUDA(cudaMemcpy((void *)j.npl, h.npl.data(), H * 4, cudaMemcpyHostToDevice));
+        PFB_CUDA(cudaMemcpy((void *)j.nl, h.nl.data(), H * 4, cudaMemcpyHostToDevice));
+        // working forms of 1 and N - 1: R mod N and N - (R mod N)
+        const pfb::big::Words N = pfb::big::from_u16(nums[i].limbs, (size_t)n_limbs);
+        const pfb::big::Words r = pfb::big::from_limbs(h.x0.data(), LIMB_BITS, H);
+        const std::vector<uint64_t> o = widen16(r, (size_t)n_limbs), m = widen16(pfb::big::sub(N, r), (size_t)n_limbs);
+        std::copy(o.begin(), o.end(), one.begin() + (size_t)i * n_limbs);
+        std::copy(m.begin(), m.end(), nm1.begin() + (size_t)i * n_limbs);
+        off += l.total;
+    }
+    PFB_CUDA(cudaMemcpy(c->d_jobs, jobs.data(), n_batch * sizeof(JobDev), cudaMemcpyHostToDevice));
+    PFB_CUDA(cudaMemcpy(c->d_ex, ex.data(), n_batch * sizeof(CtxExtra), cudaMemcpyHostToDevice));
+    PFB_CUDA(cudaMemcpy(c->d_one, one.data(), one.size() * 8, cudaMemcpyHostToDevice));
+    PFB_CUDA(cudaMemcpy(c->d_nm1, nm1.data(), nm1.size() * 8, cudaMemcpyHostToDevice));
+    const std::vector<uint64_t> nall(n16.begin(), n16.end());
+    PFB_CUDA(cudaMemcpy(c->d_n, nall.data(), nall.size() * 8, cudaMemcpyHostToDevice));
+    prep_kernel<<<n_batch, THREADS, smem_bytes(c->maxlog), e->stream>>>(c->d_jobs, nullptr, e->tw);
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(e->stream);
+    if (ce != cudaSuccess) return ctx_fail(c, pfb::cuda_fail(ce, "pfb_mr_ctx_create", __FILE__, __LINE__));
+    *out = c;
+    return PFB_OK;
+}
+
+extern "C" void pfb_mr_ctx_destroy(pfb_mr_ctx_t *c) {
+    if (!c) return;
+    cudaSetDevice(c->e->device);
+    cudaDeviceSynchronize();
+    ctx_fail(c, PFB_OK);
+}
+
+extern "C" int pfb_mr_ctx_n_sum(const pfb_mr_ctx_t *c) { return c ? 2 * c->n16 + 16 : -1; }
+
+extern "C" int pfb_mr_ctx_buffers(const pfb_mr_ctx_t *c, const uint64_t **d_N, const uint64_t **d_one,
+                                  const uint64_t **d_nm1) {
+    if (!c) {
+        pfb::set_error("pfb_mr_ctx_buffers: null context");
+        return PFB_E_ARG;
+    }
+    if (d_N) *d_N = c->d_n;
+    if (d_one) *d_one = c->d_one;
+    if (d_nm1) *d_nm1 = c->d_nm1;
+    return PFB_OK;
+}
+
+extern "C" int pfb_mr_ctx_to_residue(pfb_mr_ctx_t *c, const uint64_t *x_all, uint64_t *out_all) {
+    if (!c || !x_all || !out_all) {
+        pfb::set_error("pfb_mr_ctx_to_residue: bad argument");
+        return PFB_E_ARG;
+    }
+    using namespace pfb::big;
+    std::vector<uint16_t> t(c->n16);
+    for (int i = 0; i < c->n; i++) {
+        const size_t o = (size_t)i * c->n16;
+        for (int k = 0; k < c->n16; k++) t[k] = (uint16_t)x_all[o + k];
+        const Words x = from_u16(t.data(), (size_t)c->n16);
+        const HostPrep &h = c->hp[i];
+        const Words N = from_limbs(h.nl.data(), LIMB_BITS, h.nl.size());
+        Words rem;
+        divmod(shl(x, (size_t)LIMB_BITS * h.nl.size()), N, nullptr, &rem);  // x R mod N
+        const std::vector<uint64_t> r = widen16(rem, (size_t)c->n16);
+        std::copy(r.begin(), r.end(), out_all + o);
+    }
+    return PFB_OK;
+}
+
+extern "C" int pfb_mr_ctx_from_residue(pfb_mr_ctx_t *c, const uint64_t *d_x, uint64_t *out_all) {
+    if (!out_all) {
+        pfb::set_error("pfb_mr_ctx_from_residue: bad argument");
+        return PFB_E_ARG;
+    }
+    const int rc = ctx_launch(c, d_x, nullptr, c ? c->d_tmp : nullptr, c ? c->n16 : 0, CTX_FROM, nullptr);
+    if (rc) return rc;
+    PFB_CUDA(cudaMemcpyAsync(out_all, c->d_tmp, (size_t)c->n * c->n16 * 8, cudaMemcpyDeviceToHost, c->e->stream));
+    PFB_CUDA(cudaStreamSynchronize(c->e->stream));
+    return PFB_OK;
+}
+
+extern "C" int pfb_mr_ctx_check_passed(pfb_mr_ctx_t *c, const uint64_t *d_r, uint8_t *d_passed, void *stream) {
+    if (!c || !d_r || !d_passed) {
+        pfb::set_error("pfb_mr_ctx_check_passed: bad argument");
+        return PFB_E_ARG;
+    }
+    PFB_CUDA(cudaSetDevice(c->e->device));
+    cudaStream_t st = stream ? (cudaStream_t)stream : c->e->stream;
+    ctx_check_kernel<<<c->n, 256, 0, st>>>(d_r, c->d_one, c->d_nm1, d_passed, c->n16);
+    PFB_CUDA(cudaGetLastError());
+    return PFB_OK;
+}
+
+extern "C" int pfb_mr_ctx_modsq(pfb_mr_ctx_t *c, const uint64_t *d_a, uint64_t *d_out, void *stream) {
+    return ctx_launch(c, d_a, nullptr, d_out, c ? c->n16 : 0, CTX_MODSQ, stream);
+}
+
+extern "C" int pfb_mr_ctx_modmul(pfb_mr_ctx_t *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out,
+                                 void *stream) {
+    return ctx_launch(c, d_a, d_b, d_out, c ? c->n16 : 0, CTX_MODMUL, stream);
+}
+
+extern "C" int pfb_mr_ctx_sq_raw(pfb_mr_ctx_t *c, const uint64_t *d_a, uint64_t *d_out, void *stream) {
+    return ctx_launch(c, d_a, nullptr, d_out, c ? 2 * c->n16 + 16 : 0, CTX_RAW_SQ, stream);
+}
+
+extern "C" int pfb_mr_ctx_mul_raw(pfb_mr_ctx_t *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out,
+                                  void *stream) {
+    return ctx_launch(c, d_a, d_b, d_out, c ? 2 * c->n16 + 16 : 0, CTX_RAW_MUL, stream);
 }

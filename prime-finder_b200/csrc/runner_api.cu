@@ -18,7 +18,7 @@
 #include "pfb_mr.h"
 
 BatchModCtx::BatchModCtx(const std::vector<uint64_t> &N_all, int n_limbs_, int n_batch_, int device_id_)
-    : n_limbs(n_limbs_), n_batch(n_batch_), device_id(device_id_) {
+    : n_limbs(n_limbs_), n_batch(n_batch_), n_sum(2 * n_limbs_ + 16), device_id(device_id_) {
     if (n_limbs <= 0 || n_batch <= 0 || N_all.size() < (size_t)n_limbs * (size_t)n_batch)
         throw std::runtime_error("BatchModCtx: N_all holds fewer than n_batch * n_limbs limbs");
     N16.resize((size_t)n_limbs * n_batch);
@@ -28,9 +28,60 @@ BatchModCtx::BatchModCtx(const std::vector<uint64_t> &N_all, int n_limbs_, int n
     }
     if (pfb_mr_create(&engine, device_id) != PFB_OK)
         throw std::runtime_error(std::string("BatchModCtx: ") + pfb_last_error());
+    if (pfb_mr_ctx_create(engine, N_all.data(), n_limbs, n_batch, &ctx) != PFB_OK ||
+        pfb_mr_ctx_buffers(ctx, &d_N, &d_one_res, &d_Nm1_res) != PFB_OK) {
+        const std::string msg = std::string("BatchModCtx: ") + pfb_last_error();
+        pfb_mr_ctx_destroy(ctx);
+        pfb_mr_destroy(engine);
+        throw std::runtime_error(msg);
+    }
 }
 
-BatchModCtx::~BatchModCtx() { pfb_mr_destroy(engine); }
+BatchModCtx::~BatchModCtx() {
+    pfb_mr_ctx_destroy(ctx);
+    pfb_mr_destroy(engine);
+}
+
+namespace {
+
+void ctx_check(int rc, const char *what) {
+    if (rc != PFB_OK) throw std::runtime_error(std::string(what) + ": " + pfb_last_error());
+}
+
+}  // namespace
+
+void BatchModCtx::to_residue_batch(const std::vector<uint64_t> &x_all, std::vector<uint64_t> &out_all) const {
+    if (x_all.size() < (size_t)n_batch * n_limbs) throw std::runtime_error("to_residue_batch: x_all too short");
+    out_all.assign((size_t)n_batch * n_limbs, 0);
+    ctx_check(pfb_mr_ctx_to_residue(ctx, x_all.data(), out_all.data()), "to_residue_batch");
+}
+
+void BatchModCtx::from_residue_batch(const Data64 *d_x, std::vector<uint64_t> &out_all) const {
+    out_all.assign((size_t)n_batch * n_limbs, 0);
+    ctx_check(pfb_mr_ctx_from_residue(ctx, d_x, out_all.data()), "from_residue_batch");
+}
+
+void BatchModCtx::check_passed(const Data64 *d_r_mont, uint8_t *d_passed, cudaStream_t s) const {
+    ctx_check(pfb_mr_ctx_check_passed(ctx, d_r_mont, d_passed, s), "check_passed");
+}
+
+void BatchModCtx::modmul_batch(const Data64 *d_A, const Data64 *d_B, Data64 *d_out, cudaStream_t s) {
+    ctx_check(pfb_mr_ctx_modmul(ctx, d_A, d_B, d_out, s), "modmul_batch");
+}
+
+void BatchModCtx::modsq_batch(const Data64 *d_A, Data64 *d_out, cudaStream_t s) {
+    ctx_check(pfb_mr_ctx_modsq(ctx, d_A, d_out, s), "modsq_batch");
+}
+
+void BatchModCtx::mul_no_redc_batch(const Data64 *d_A, const Data64 *d_B, Data64 *d_out, cudaStream_t s) {
+    ctx_check(pfb_mr_ctx_mul_raw(ctx, d_A, d_B, d_out, s), "mul_no_redc_batch");
+    ctx_check(cudaStreamSynchronize(s) == cudaSuccess ? PFB_OK : PFB_E_CUDA, "mul_no_redc_batch");
+}
+
+void BatchModCtx::sq_no_redc_batch(const Data64 *d_A, Data64 *d_out, cudaStream_t s) {
+    ctx_check(pfb_mr_ctx_sq_raw(ctx, d_A, d_out, s), "sq_no_redc_batch");
+    ctx_check(cudaStreamSynchronize(s) == cudaSuccess ? PFB_OK : PFB_E_CUDA, "sq_no_redc_batch");
+}
 
 namespace {
 
