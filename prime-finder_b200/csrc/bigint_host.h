@@ -319,6 +319,148 @@ inline Words sub(const Words &a, const Words &b) {
     return r;
 }
 
+// r = a * x - b * y for a * x >= b * y (a, b single words); r is reused.
+inline void mulsub_small(Words &r, const Words &x, uint64_t a, const Words &y, uint64_t b) {
+    const size_t n = std::max(x.size(), y.size()) + 1;
+    r.assign(n, 0);
+    unsigned __int128 cx = 0, cy = 0;
+    uint64_t borrow = 0;
+    for (size_t i = 0; i < n; i++) {
+        cx += (unsigned __int128)(i < x.size() ? x[i] : 0) * a;
+        cy += (unsigned __int128)(i < y.size() ? y[i] : 0) * b;
+        const uint64_t px = (uint64_t)cx, py = (uint64_t)cy;
+        cx >>= 64;
+        cy >>= 64;
+        const unsigned __int128 d = (unsigned __int128)px - py - borrow;
+        r[i] = (uint64_t)d;
+        borrow = (uint64_t)(d >> 127);
+    }
+    trim(r);
+}
+
+// r = a * x + b * y (a, b single words); r is reused.
+inline void muladd_small(Words &r, const Words &x, uint64_t a, const Words &y, uint64_t b) {
+    const size_t n = std::max(x.size(), y.size()) + 2;
+    r.assign(n, 0);
+    unsigned __int128 cx = 0, cy = 0, c = 0;
+    for (size_t i = 0; i < n; i++) {
+        cx += (unsigned __int128)(i < x.size() ? x[i] : 0) * a;
+        cy += (unsigned __int128)(i < y.size() ? y[i] : 0) * b;
+        c += (unsigned __int128)(uint64_t)cx + (uint64_t)cy;
+        cx >>= 64;
+        cy >>= 64;
+        r[i] = (uint64_t)c;
+        c >>= 64;
+    }
+    trim(r);
+}
+
+inline Words add(const Words &a, const Words &b) {
+    Words r(std::max(a.size(), b.size()) + 1, 0);
+    unsigned __int128 c = 0;
+    for (size_t i = 0; i < r.size(); i++) {
+        c += (unsigned __int128)(i < a.size() ? a[i] : 0) + (i < b.size() ? b[i] : 0);
+        r[i] = (uint64_t)c;
+        c >>= 64;
+    }
+    trim(r);
+    return r;
+}
+
+// Bits sh .. sh + 127 of x.
+inline unsigned __int128 bits128(const Words &x, size_t sh) {
+    const size_t w = sh / 64, b = sh % 64;
+    auto at = [&](size_t i) -> uint64_t { return i < x.size() ? x[i] : 0; };
+    const uint64_t w0 = at(w), w1 = at(w + 1), w2 = at(w + 2);
+    const uint64_t lo = b ? (w0 >> b) | (w1 << (64 - b)) : w0;
+    const uint64_t hi = b ? (w1 >> b) | (w2 << (64 - b)) : w1;
+    return ((unsigned __int128)hi << 64) | lo;
+}
+
+// a^-1 mod M (0 < a < M) by Lehmer's extended Euclid (Knuth, TAOCP vol. 2,
+// 4.5.2, Algorithm L) on 126-bit leading parts, with single-precision
+// cofactors kept below 2^62.  Only the cofactor of a is kept, as a
+// magnitude and a sign: the remainders u, v satisfy u == tu a, v == tv a
+// (mod M), and tu, tv alternate in sign, so every cofactor update adds
+// magnitudes.  Returns false when gcd(a, M) != 1.
+inline bool inv_mod(const Words &a, const Words &M, Words *inv) {
+    Words u = M, v = a, tu, tv(1, 1), u2, v2, t1, t2;
+    trim(v);
+    int su = -1, sv = 1;  // signs of tu (zero: either) and tv
+    const __int128 LIM = (__int128)1 << 62;
+    while (!v.empty()) {
+        const size_t h = bit_length(u);
+        if (h <= 64) {  // single precision to the end
+            uint64_t x = u[0], y = v[0];
+            while (y) {
+                const uint64_t q = x / y, r = x - q * y;
+                Words t = add(tu, mul_small(tv, q));  // tu - q tv, magnitude; sign su
+                tu = std::move(tv);
+                tv = std::move(t);
+                std::swap(su, sv);
+                x = y;
+                y = r;
+            }
+            u = Words(1, x);
+            trim(u);
+            v.clear();
+            break;
+        }
+        const size_t sh = h > 126 ? h - 126 : 0;
+        __int128 uu = (__int128)bits128(u, sh), vv = (__int128)bits128(v, sh);
+        __int128 A = 1, B = 0, C = 0, D = 1;
+        while (vv + C != 0 && vv + D != 0) {
+            const __int128 q = (uu + A) / (vv + C);
+            if (q != (uu + B) / (vv + D)) break;
+            const __int128 nC = A - q * C, nD = B - q * D;
+            if (nC > LIM || nC < -LIM || nD > LIM || nD < -LIM) break;
+            A = C;
+            C = nC;
+            B = D;
+            D = nD;
+            const __int128 t = uu - q * vv;
+            uu = vv;
+            vv = t;
+        }
+        if (B == 0) {  // no single-precision step was certain: one full division
+            Words q, r;
+            divmod(u, v, &q, &r);
+            Words t = add(tu, mul(tv, q));
+            tu = std::move(tv);
+            tv = std::move(t);
+            std::swap(su, sv);
+            u = std::move(v);
+            v = std::move(r);
+            continue;
+        }
+        auto mag = [](__int128 x) { return (uint64_t)(x < 0 ? -x : x); };
+        // u' = A u + B v, v' = C u + D v (A, B and C, D of opposite signs or
+        // zero, u', v' >= 0): the positive term is the one of the
+        // non-positive partner's sign opposite (A = 0 after a single step)
+        if (B <= 0) mulsub_small(u2, u, mag(A), v, mag(B));
+        else mulsub_small(u2, v, mag(B), u, mag(A));
+        if (D <= 0) mulsub_small(v2, u, mag(C), v, mag(D));
+        else mulsub_small(v2, v, mag(D), u, mag(C));
+        // cofactors: A tu and B tv have one sign, as have C tu and D tv
+        const int s1 = A != 0 ? (A > 0 ? su : -su) : (B > 0 ? sv : -sv);
+        const int s2 = C != 0 ? (C > 0 ? su : -su) : (D > 0 ? sv : -sv);
+        muladd_small(t1, tu, mag(A), tv, mag(B));
+        muladd_small(t2, tu, mag(C), tv, mag(D));
+        std::swap(u, u2);
+        std::swap(v, v2);
+        std::swap(tu, t1);
+        std::swap(tv, t2);
+        su = s1;
+        sv = s2;
+    }
+    if (!(u.size() == 1 && u[0] == 1)) return false;
+    Words r;
+    divmod(tu, M, nullptr, &r);
+    if (su < 0 && !r.empty()) r = sub(M, r);
+    *inv = r;
+    return true;
+}
+
 // floor(sqrt(a)) by Newton's iteration from a power of two above the root.
 inline Words isqrt(const Words &a) {
     const size_t bits = bit_length(a);

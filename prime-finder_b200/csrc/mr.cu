@@ -120,10 +120,10 @@ namespace {
 
 // Per-candidate device layout inside the arena (32-bit words).
 struct Layout {
-    size_t x, res, nph, nh, npl, nl, exp, ss, st, yb, lv0, lv1, lqk, lt, lone, gy, total;
+    size_t x, res, nn, nh, npl, nl, exp, yb, lv0, lv1, lqk, lt, lone, gy, raw, total;
 };
 
-Layout layout_for(int logl, size_t exp_words, bool lucas = false) {
+Layout layout_for(int logl, size_t exp_words, bool lucas = false, bool raw = false) {
     const size_t L = (size_t)1 << logl, H = L / 2;
     Layout l{};
     size_t o = 0;
@@ -134,16 +134,12 @@ Layout layout_for(int logl, size_t exp_words, bool lucas = false) {
     };
     l.x = take(H);
     l.res = take(H);
-    l.nph = take(2 * L);
+    l.nn = take(2 * H);
     l.nh = take(2 * H);
     l.npl = take(H);
     l.nl = take(H);
     l.exp = take(exp_words);
-    if (logl > LOG_LCTA) {
-        l.ss = take(L);
-        l.st = take(H);
-        l.yb = take(H + H / 32);  // padded like the shared-memory residue
-    }
+    if (logl > LOG_LCTA) l.yb = take(H + H / 32);  // padded like the shared-memory residue
     if (lucas) {
         l.lv0 = take(H);
         l.lv1 = take(H);
@@ -152,6 +148,7 @@ Layout layout_for(int logl, size_t exp_words, bool lucas = false) {
         l.lone = take(H);
         l.gy = take(2 * L);
     }
+    if (raw) l.raw = take(2 * L);  // L 64-bit coefficients
     l.total = o;
     return l;
 }
@@ -317,16 +314,12 @@ int batch_build(pfb_mr *e, const pfb_mr_number_t *nums, int n, uint32_t base, in
         const Layout &l = lay[i];
         j.x = w + l.x;
         j.res = w + l.res;
-        j.nph = w + l.nph;
+        j.nn = w + l.nn;
         j.nh = w + l.nh;
         j.npl = w + l.npl;
         j.nl = w + l.nl;
         j.exp = w + l.exp;
-        if (h.logl > LOG_LCTA) {
-            j.spill_s = w + l.ss;
-            j.spill_t = w + l.st;
-            j.ybuf = w + l.yb;
-        }
+        if (h.logl > LOG_LCTA) j.ybuf = w + l.yb;
         j.logl = h.logl;
         j.cursor = h.cursor;
         j.extra = mode >= 1 ? h.s - 1 : 0;
@@ -900,16 +893,12 @@ int srv_admit(pfb_mr_server *s, std::vector<int> &admitted) {
         memset(&j, 0, sizeof(j));
         j.x = w + l.x;
         j.res = w + l.res;
-        j.nph = w + l.nph;
+        j.nn = w + l.nn;
         j.nh = w + l.nh;
         j.npl = w + l.npl;
         j.nl = w + l.nl;
         j.exp = w + l.exp;
-        if (h.logl > LOG_LCTA) {
-            j.spill_s = w + l.ss;
-            j.spill_t = w + l.st;
-            j.ybuf = w + l.yb;
-        }
+        if (h.logl > LOG_LCTA) j.ybuf = w + l.yb;
         j.logl = h.logl;
         j.cursor = h.cursor;
         j.extra = h.s - 1;
@@ -1238,7 +1227,7 @@ extern "C" int pfb_mr_ctx_create(pfb_mr_t *e, const uint64_t *N_all, int n_limbs
             pfb::set_error("pfb_mr_ctx_create: modulus %d is not odd, > 1 and at most %d bits", i, PFB_MR_MAX_BITS);
             return ctx_fail(c, PFB_E_ARG);
         }
-        lay[i] = layout_for(c->hp[i].logl, 1, true);  // the Lucas layout: gy [2][L] and spare H-word buffers
+        lay[i] = layout_for(c->hp[i].logl, 1, true, true);  // gy [2][L], spare H-word buffers, raw coefficients
         words += lay[i].total;
         c->maxlog = std::max(c->maxlog, c->hp[i].logl);
     }
@@ -1268,21 +1257,18 @@ extern "C" int pfb_mr_ctx_create(pfb_mr_t *e, const uint64_t *N_all, int n_limbs
         uint32_t *w = d_words + off;
         JobDev &j = jobs[i];
         memset(&j, 0, sizeof(j));
-        j.nph = w + l.nph;
+        j.nn = w + l.nn;
         j.nh = w + l.nh;
         j.npl = w + l.npl;
         j.nl = w + l.nl;
         j.x = w + l.x;
         j.res = w + l.res;
-        if (h.logl > LOG_LCTA) {
-            j.spill_s = w + l.ss;
-            j.spill_t = w + l.st;
-            j.ybuf = w + l.yb;
-        }
+        if (h.logl > LOG_LCTA) j.ybuf = w + l.yb;
         j.logl = h.logl;
         j.phase = 0;
         ex[i].gy = w + l.gy;
         ex[i].yl = w + l.lt;
+        ex[i].raw = (unsigned long long *)(w + l.raw);
         const size_t H = h.nl.size();
         PFB_CUDA(cudaMemcpy((void *)j.npl, h.npl.data(), H * 4, cudaMemcpyHostToDevice));
         PFB_CUDA(cudaMemcpy((void *)j.nl, h.nl.data(), H * 4, cudaMemcpyHostToDevice));
@@ -1343,7 +1329,7 @@ extern "C" int pfb_mr_ctx_to_residue(pfb_mr_ctx_t *c, const uint64_t *x_all, uin
         const HostPrep &h = c->hp[i];
         const Words N = from_limbs(h.nl.data(), LIMB_BITS, h.nl.size());
         Words rem;
-        divmod(shl(x, (size_t)LIMB_BITS * h.nl.size()), N, nullptr, &rem);  // x R mod N
+        divmod(add(shl(x, (size_t)LIMB_BITS * h.nl.size()), x), N, nullptr, &rem);  // x R' mod N, R' = 2^(22 H) + 1
         const std::vector<uint64_t> r = widen16(rem, (size_t)c->n16);
         std::copy(r.begin(), r.end(), out_all + o);
     }

@@ -4,8 +4,8 @@
 // operands in the reference's layout -- 16-bit limbs, one per uint64 --
 // instead of a whole exponentiation.
 //
-// Working form ("residue"): x R mod N, fully reduced (< N), R = 2^(22 H) of
-// the modulus' transform length; the same numbers the engine keeps
+// Working form ("residue"): x R' mod N, fully reduced (< N), R' = 2^(22 H) + 1
+// of the modulus' transform length; the same numbers the engine keeps
 // internally in 22-bit limbs, before its final conditional subtraction.
 #pragma once
 #include <cuda_runtime.h>
@@ -27,8 +27,9 @@ enum CtxOp : int {
 // Per-modulus buffers beyond the engine's own (JobDev: spectra of N' and N,
 // limbs of N, spill buffers of the longest transform).
 struct CtxExtra {
-    uint32_t *gy;  // [2][L] spectrum of the second factor
-    uint32_t *yl;  // H limbs of the second factor
+    uint32_t *gy;              // [2][L] spectrum of the second factor
+    uint32_t *yl;              // H limbs of the second factor
+    unsigned long long *raw;   // L coefficients of a raw product
 };
 
 // 16-bit limbs (one per uint64, the reference's Data64 layout) -> H limbs of
@@ -70,54 +71,48 @@ __device__ __forceinline__ void cond_sub_n(uint32_t *X, uint32_t *T, const uint3
 }
 
 // The full product X Y (gy: the spectrum of Y) or X^2 of the H limbs in
-// sm.X, as L limbs of 22 bits in sm.A0 (padded); no reduction.
+// sm.X, as L limbs of 22 bits in A0..A1 read as one padded array of L words
+// (A1 follows A0); no reduction.  With T(z) = A(z) + z^H C(z) the cyclic
+// product gives c = A + C and the negacyclic one d = A - C, coefficient by
+// coefficient, so T's coefficients are (c + d) / 2 and (c - d) / 2, both
+// exact; raw holds the 2H coefficients between the products and the carry.
 template <int LOGL>
-__device__ void raw_product_t(const Smem &sm, const JobDev &jb, bool square, const uint32_t *gy,
+__device__ void raw_product_t(const Smem &sm, bool square, const uint32_t *gy, unsigned long long *raw,
                               const Twiddles &tw) {
-    constexpr int L = 1 << LOGL, H = L >> 1;
+    constexpr int L = 1 << LOGL, H = L >> 1, LOGH = LOGL - 1;
     const int tid = threadIdx.x;
-    CarrySmem &cs = *sm.cs;
-    if constexpr (LOGL <= LOG_LCTA) {
-        for (int i = tid; i < H; i += THREADS) {
-            const uint32_t v = sm.X[pad(i)];
-            sm.A0[pad(i)] = v;
-            sm.A1[pad(i)] = v;
-        }
-        __syncthreads();
-        if (square) product_from<true, 0, LOGL, 0, false, true>(sm.A0, sm.A1, tw, nullptr, nullptr, c_crt);
-        else product_from<true, 0, LOGL, 1, true, true>(sm.A0, sm.A1, tw, gy, gy + L, c_crt);
-        carry_pass<true>(L, 0ull, [&](int i) { return crt(sm.A0[pad(i)], sm.A1[pad(i)], LOGL, c_crt); }, sm.A0,
-                         cs);
-    } else {
-        // one prime after the other; the p1 coefficients make a round trip
-        // through the spill buffer in the order the CRT's carry pass reads them
-        uint32_t *A = sm.A0;
-        for (int i = tid; i < H; i += THREADS) A[pad(i)] = sm.X[pad(i)];
-        __syncthreads();
-        if (square) product_from<false, 0, LOGL, 0, false, true>(A, nullptr, tw, nullptr, nullptr, c_crt);
-        else product_from<false, 0, LOGL, 1, true, true>(A, nullptr, tw, gy, nullptr, c_crt);
-        constexpr int W = L / THREADS;
-        for (int j = tid; j < L; j += THREADS) jb.spill_s[j] = A[pad((j % THREADS) * W + j / THREADS)];
-        __syncthreads();
-        for (int i = tid; i < H; i += THREADS) A[pad(i)] = sm.X[pad(i)];
-        __syncthreads();
-        if (square) product_from<false, 1, LOGL, 0, false, true>(A, nullptr, tw, nullptr, nullptr, c_crt);
-        else product_from<false, 1, LOGL, 1, true, true>(A, nullptr, tw, gy + L, nullptr, c_crt);
-        carry_pass<true>(
-            L, 0ull,
-            [&](int i) { return crt(ldg_spill(jb.spill_s + spill_slot<L>(i)), A[pad(i)], LOGL, c_crt); }, A, cs);
+    uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
+    for (int i = tid; i < H; i += THREADS) {
+        const uint32_t v = X[pad(i)];
+        A0[pad(i)] = v;
+        A1[pad(i)] = v;
     }
+    __syncthreads();
+    if (square) product_from<true, 0, LOGH, 0, false>(A0, A1, tw, nullptr, nullptr, c_crt);
+    else product_from<true, 0, LOGH, 1, true>(A0, A1, tw, gy, gy + L, c_crt);
+    for (int i = tid; i < H; i += THREADS) raw[i] = crt(A0[pad(i)], A1[pad(i)], LOGH, c_crt);
+    for (int i = tid; i < H; i += THREADS) {
+        const uint32_t v = X[pad(i)];
+        X[pad(i)] = twist<LOGL, 0>(v, i, tw);
+        A1[pad(i)] = twist<LOGL, 1>(v, i, tw);
+    }
+    __syncthreads();
+    if (square) product_from<true, 0, LOGH, 0, false>(X, A1, tw, nullptr, nullptr, c_crt);
+    else product_from<true, 0, LOGH, 1, true>(X, A1, tw, gy + H, gy + L + H, c_crt);
+    for (int i = tid; i < H; i += THREADS)  // d as a two's-complement 64-bit value
+        raw[H + i] = crt_signed(untwist<LOGL, 0>(X[pad(i)], i, tw), untwist<LOGL, 1>(A1[pad(i)], i, tw), LOGH,
+                                c_crt, 0ull);
+    __syncthreads();
+    carry_pass<true>(L, 0ull, [&](int i) {
+        const int k = i < H ? i : i - H;
+        const long long c = (long long)raw[k], d = (long long)raw[H + k];
+        return (unsigned long long)((i < H ? c + d : c - d) >> 1);
+    }, A0, *sm.cs);
 }
 
-__device__ void raw_product(const Smem &sm, const JobDev &jb, bool square, const uint32_t *gy, const Twiddles &tw) {
-    switch (jb.logl) {
-#define PFB_RAW(n)                                     \
-    case n:                                            \
-        raw_product_t<n>(sm, jb, square, gy, tw);      \
-        break;
-        PFB_RAW(8) PFB_RAW(9) PFB_RAW(10) PFB_RAW(11) PFB_RAW(12) PFB_RAW(13) PFB_RAW(14) PFB_RAW(15)
-#undef PFB_RAW
-    }
+__device__ void raw_product(const Smem &sm, int logl, bool square, const uint32_t *gy, unsigned long long *raw,
+                            const Twiddles &tw) {
+    PFB_LOGL_SWITCH(logl, (raw_product_t<LG>(sm, square, gy, raw, tw)))
 }
 
 // One operation on every modulus of a context: CTA b takes modulus b, its
@@ -133,7 +128,7 @@ ctx_kernel(const JobDev *jobs, const CtxExtra *ex, const uint64_t *A, const uint
     uint32_t *Y;
     carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int L = 1 << jb.logl, H = L >> 1;
-    const Cand cd{jb.nph, jb.nh, jb.logl};
+    const Cand cd{jb.nn, jb.nh, jb.logl};
     const CtxExtra e = ex[blockIdx.x];
     const size_t b = blockIdx.x;
     uint64_t *o = out + b * (size_t)out_stride;
@@ -154,7 +149,7 @@ ctx_kernel(const JobDev *jobs, const CtxExtra *ex, const uint64_t *A, const uint
         break;
     case CTX_RAW_SQ:
     case CTX_RAW_MUL:
-        raw_product(sm, jb, op == CTX_RAW_SQ, e.gy, tw);
+        raw_product(sm, jb.logl, op == CTX_RAW_SQ, e.gy, e.raw, tw);
         __syncthreads();
         store16(o, sm.A0, L, out_stride);
         break;

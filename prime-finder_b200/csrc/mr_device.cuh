@@ -3,18 +3,18 @@
 //
 // Replaces the reference's per-squaring chain of ~39 launches
 // (batch_mod_ctx.cu:288-316 -> ntt_4step.cu:202-295 -> carry_norm.cu:63-122
-// -> barrett.cu:128-199 / sub.cu:18-155) with one CTA-resident sequence:
+// -> barrett.cu:128-199 / sub.cu:18-155) with one CTA-resident sequence of
+// four length-H products (x of H limbs of 22 bits, B = 2^22, Montgomery radix
+// R' = B^H + 1; see mont_step):
 //
-//   x (H limbs of 22 bits, x < 4N)          R = 2^(22*H), L = 2H
-//   T  = x^2                  cyclic NTT of length L over p1 and p2, CRT
-//   m  = (T mod R) * N' mod R length-L NTT product with the stored NTT(N')
-//   W  = m * N mod (R - 1)    length-H cyclic NTT product with the stored NTT(N)
-//   U  = (T_lo + T_hi + W) mod (R - 1)
+//   S = x^2 mod (B^H - 1)     cyclic NTT of length H over p1 and p2, CRT
+//   D = x^2 mod (B^H + 1)     negacyclic NTT of length H
+//   m = D N'' mod (B^H + 1)   negacyclic product with the stored NTT of N''
+//   W = m N mod (B^H - 1)     cyclic product with the stored NTT of N
+//   2 REDC(x^2) = S + W mod (B^H - 1)
 //
-// U equals (T + m N) / R (Montgomery's REDC): T + mN == 0 (mod R), and
-// modulo R - 1 the quotient by R is the sum of the halves; 0 <= U < 2N < R-1
-// makes the residue exact.  Exact 30-bit modular butterflies (Shoup's
-// multiplication, Harvey's lazy [0, 2p) ranges) run on the integer pipe.
+// Exact 30-bit modular butterflies (Shoup's multiplication, Harvey's lazy
+// [0, 2p) ranges) run on the integer pipe.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -575,159 +575,169 @@ __device__ __forceinline__ void pointwise2(uint32_t *A0, uint32_t *A1, const uin
 
 // Per-CTA view of one candidate.
 struct Cand {
-    const uint32_t *nph;   // NTT_L(N')  [2][L] (bit-reversed spectral order)
-    const uint32_t *nh;    // NTT_H(N)   [2][H]
+    const uint32_t *nn;    // NTT of N'' = -N^-1 mod (B^H + 1), negacyclic, [2][H]
+    const uint32_t *nh;    // NTT_H(N), cyclic, [2][H]
     int logl;
 };
 
+// Shared-memory view of one step: three transform buffers of H padded words
+// (A0, A1, X; X holds the residue between steps) and the carry scratch.
 struct Smem {
     uint32_t *A0, *A1, *X;
     CarrySmem *cs;
 };
 
-// One Montgomery step on X (H limbs): X <- REDC(X^2) * a   (square = true)
-//                                   or X <- REDC(X * Y) * a  (gy = spectrum of Y)
-//                                   or X <- REDC(X)           (square = false).
-// gy holds NTT_L(Y) of both primes ([2][L], reduced), written earlier in the
-// same launch.  On entry X, Y < B N with R > B^2 N (B = 4 for the strong
-// test's squarings), or X < R for a plain REDC; on exit X < 2N * a.
-// MUL = false compiles the squaring / REDC forms only (gy ignored).
+// Negacyclic transforms of length H are cyclic ones of the input twisted by
+// psi^i, psi = omega_L a primitive 2H-th root of unity (the upper half of
+// the length-L transform of a zero-padded input); the inverse untwists by
+// psi^-i.  psi^i = w[i 2^(LOG_LMAX - LOGL)], within the table's half circle.
+template <int LOGL, int PR>
+__device__ __forceinline__ uint32_t twist(uint32_t v, int i, const Twiddles &tw) {
+    const int k = i << (LOG_LMAX - LOGL);
+    return shoup(v, __ldg(tw.w[PR] + k), __ldg(tw.wsh[PR] + k), PR ? P2 : P1);
+}
+
+template <int LOGL, int PR>
+__device__ __forceinline__ uint32_t untwist(uint32_t v, int i, const Twiddles &tw) {
+    const int k = i << (LOG_LMAX - LOGL);
+    return shoup(v, __ldg(tw.wi[PR] + k), __ldg(tw.wish[PR] + k), PR ? P2 : P1);
+}
+
+// Signed coefficients.  A product of two H-coefficient operands with limbs in
+// (-2^22, 2^22 + 2) has coefficients c with |c| < H 2^44 (1 + 2^-20) < P12/2
+// (H <= 2^14); the CRT gives c mod P12.  Adding OFF_i >= 2^59 - 2^37 to
+// position i makes every coefficient non-negative for the carry pass, and
+// the offsets sum to a multiple of the modulus the product lives in:
+//   cyclic (mod B^H - 1):     OFF_i = 2^37 (B - 1)                sum 2^37 (B^H - 1)
+//   negacyclic (mod B^H + 1): OFF_0 = 2^37 (B + 1), OFF_i = 2^37 (B - 1)   sum 2^37 (B^H + 1)
+constexpr unsigned long long P12 = (unsigned long long)P1 * P2;
+constexpr unsigned long long OFF_C = (1ull << 37) * ((1ull << LIMB_BITS) - 1ull);
+constexpr unsigned long long OFF_N0 = (1ull << 37) * ((1ull << LIMB_BITS) + 1ull);
+
+__device__ __forceinline__ unsigned long long crt_signed(uint32_t r1, uint32_t r2, int logn, const CrtConsts &cc,
+                                                         unsigned long long off) {
+    const unsigned long long v = crt(r1, r2, logn, cc);
+    return v + off - (v > P12 / 2 ? P12 : 0ull);
+}
+
+// One Montgomery step on X (H limbs of 22 bits), with the Montgomery radix
+// R' = B^H + 1 (B = 2^22):
+//   X <- REDC(X^2) * a      (square = true)
+//   X <- REDC(X * Y) * a    (gy = spectrum of Y: cyclic half and negacyclic half, see spectrum)
+//   X <- REDC(X) * a        (square = false, no gy)
+// REDC(T) = (T + m N) / R' with m = -T N^-1 mod R' in [0, R').  Every
+// product is of length H, both primes in shared memory at once:
+//   S = T mod (B^H - 1)     cyclic square (or product)
+//   D = T mod (B^H + 1)     negacyclic square (or product)
+//   m = D N'' mod (B^H + 1) negacyclic product with the stored spectrum of N''
+//   W = m N mod (B^H - 1)   cyclic product with the stored spectrum of N
+//   V = S + W mod (B^H - 1)
+// Since R' == 2 (mod B^H - 1), V == 2 U for U = REDC(T); U < 2N and 4N <
+// B^H - 1 make V = 2U exactly, so a U is (a/2) V for even a (the base-2
+// ladder's multiply by 2 costs nothing) and a (V >> 1) for odd a.  That is 4
+// length-L-equivalent transforms per step where a radix R = B^H needs 5 (its
+// m = (T mod R) N' mod R is a zero-padded length-L product).
+// On entry X, Y < c N with R' > 4 c^2 N (c = 4 for the strong test), or
+// X < R' for a plain REDC; on exit X < 2N * a.  A1 and A0 are clobbered.
 template <bool MUL, int LOGL>
 __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
                           const CrtConsts &cc, const uint32_t *gy = nullptr) {
-    constexpr int logl = LOGL, L = 1 << logl, H = L >> 1;
+    constexpr int L = 1 << LOGL, H = L >> 1, LOGH = LOGL - 1;
+    constexpr int T = THREADS;
     uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
     CarrySmem &cs = *sm.cs;
-    const int tid = threadIdx.x, T = blockDim.x;
-    unsigned long long cS = 0;  // carry of T_lo + T_hi
-
-    // the operands of the two length-L products are H limbs, zero above:
-    // only the lower halves are stored (the first forward pass takes the
-    // upper halves as zero)
-    for (int i = tid; i < H; i += T) {
-        const uint32_t v = X[pad(i)];
-        A0[pad(i)] = v;
-        A1[pad(i)] = v;
-    }
-    __syncthreads();
-    if (square || (MUL && gy)) {
-        if (MUL && gy) product_from<true, 0, LOGL, 1, true, true>(A0, A1, tw, gy, gy + L, cc);
-        else product_from<true, 0, LOGL, 0, false, true>(A0, A1, tw, nullptr, nullptr, cc);
-        // T = x^2 (or x y) as L limbs, in place over A0
-        carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
-        // S1 = T_lo + T_hi  -> X, carry cS
-        cS = carry_pass<true>(H, 0ull,
-                               [&](int i) { return (unsigned long long)A0[pad(i)] + A0[pad(i + H)]; }, X, cs);
-        for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
-        __syncthreads();
-    }
-    // m = T_lo * N' mod R
-    product_from<true, 0, LOGL, 1, false, true>(A0, A1, tw, cd.nph, cd.nph + L, cc);
-    carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl, cc); }, A0, cs);
-    for (int i = tid; i < H; i += T) A1[pad(i)] = A0[pad(i)];
-    __syncthreads();
-    // W = m * N mod (R - 1): cyclic product of length H
-    product_from<true, 0, LOGL - 1, 1, false>(A0, A1, tw, cd.nh, cd.nh + H, cc);
-    const unsigned long long cW =
-        carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], logl - 1, cc); }, A0, cs);
-    // U = S1 + W (mod R - 1); S1 = X (square = false: S1 = x itself)
-    unsigned long long c = carry_pass<true>(
-        H, cS + cW, [&](int i) { return (unsigned long long)X[pad(i)] + A0[pad(i)]; }, X, cs);
-    while (c) {  // end-around carry: B^H == 1 (mod R - 1); at most two rounds
-        c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
-    }
-    if (a > 1u) {
-        carry_pass<true>(H, 0ull, [&](int i) { return (unsigned long long)X[pad(i)] * a; }, X, cs);
-    }
-}
-
-// Global scratch of the sequential-prime step (one per resident candidate).
-struct Spill {
-    uint32_t *s;   // L words: prime-1 inverse transform, read back by the CRT
-    uint32_t *t;   // H words: T mod R, then m
-};
-
-// Layout of the spilled prime-1 coefficients of an n-point product, n >= 2T:
-// the CRT's carry pass gives thread t the w = n/T consecutive positions
-// t w .. t w + w - 1, so position t w + q is stored at q T + t and the
-// pass's q-th reads of all threads are one coalesced line.
-template <int N>
-__device__ __forceinline__ int spill_slot(int i) {
-    constexpr int W = N / THREADS;
-    static_assert(N >= 2 * THREADS && W * THREADS == N, "carry-pass segments");
-    return (i % W) * THREADS + i / W;
-}
-
-__device__ __forceinline__ uint32_t ldg_spill(const uint32_t *p) { return __ldcg(p); }
-
-// mont_step for transforms too long for both primes to sit in shared memory
-// (L = 2^15): the p1 spectrum makes a round trip through global memory (L2).
-// Same arithmetic and result as mont_step; sm.A1 is unused.
-template <bool MUL, int LOGL>
-__device__ void mont_step_seq(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                              const CrtConsts &cc, const Spill &sp, const uint32_t *gy = nullptr) {
-    constexpr int logl = LOGL, L = 1 << logl, H = L >> 1;
-    uint32_t *A = sm.A0, *X = sm.X;
-    CarrySmem &cs = *sm.cs;
     const int tid = threadIdx.x;
-    constexpr int T = THREADS;
-    unsigned long long cS = 0;
-    // lower half of a length-L product's operand (the upper half is zero and
-    // is taken as such by the first forward pass)
-    auto load_x = [&](const uint32_t *src, bool from_global) {
-        for (int i = tid; i < H; i += T) A[pad(i)] = from_global ? ldg_spill(src + i) : src[pad(i)];
-        __syncthreads();
-    };
-    // coalesced writes: slot j holds position (j mod T) w + j / T
-    auto spill_L = [&]() {
-        constexpr int W = L / T;
-        for (int j = tid; j < L; j += T) sp.s[j] = A[pad((j % T) * W + j / T)];
-        __syncthreads();
-    };
-    auto spill_H = [&]() {
-        constexpr int W = H / T;
-        for (int j = tid; j < H; j += T) sp.s[j] = A[pad((j % T) * W + j / T)];
-        __syncthreads();
-    };
+    unsigned long long cS = 0, cD = 0;
     if (square || (MUL && gy)) {
-        load_x(X, false);
-        if (MUL && gy) product_from<false, 0, LOGL, 1, true, true>(A, nullptr, tw, gy, nullptr, cc);
-        else product_from<false, 0, LOGL, 0, false, true>(A, nullptr, tw, nullptr, nullptr, cc);
-        spill_L();
-        load_x(X, false);
-        if (MUL && gy) product_from<false, 1, LOGL, 1, true, true>(A, nullptr, tw, gy + L, nullptr, cc);
-        else product_from<false, 1, LOGL, 0, false, true>(A, nullptr, tw, nullptr, nullptr, cc);
-        carry_pass<true>(
-            L, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<L>(i)), A[pad(i)], logl, cc); }, A, cs);
-        cS = carry_pass<true>(H, 0ull,
-                               [&](int i) { return (unsigned long long)A[pad(i)] + A[pad(i + H)]; }, X, cs);
-        for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
+        // S: cyclic product, A0 (prime 1) and A1 (prime 2); carried into A0
+        for (int i = tid; i < H; i += T) {
+            const uint32_t v = X[pad(i)];
+            A0[pad(i)] = v;
+            A1[pad(i)] = v;
+        }
         __syncthreads();
+        if (MUL && gy) product_from<true, 0, LOGH, 1, true>(A0, A1, tw, gy, gy + L, cc);
+        else product_from<true, 0, LOGH, 0, false>(A0, A1, tw, nullptr, nullptr, cc);
+        cS = carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], LOGH, cc); }, A0, cs);
+        // D: negacyclic product, X itself (prime 1) and A1 (prime 2); carried into X
+        for (int i = tid; i < H; i += T) {
+            const uint32_t v = X[pad(i)];
+            X[pad(i)] = twist<LOGL, 0>(v, i, tw);
+            A1[pad(i)] = twist<LOGL, 1>(v, i, tw);
+        }
+        __syncthreads();
+        if (MUL && gy) product_from<true, 0, LOGH, 1, true>(X, A1, tw, gy + H, gy + L + H, cc);
+        else product_from<true, 0, LOGH, 0, false>(X, A1, tw, nullptr, nullptr, cc);
+        cD = carry_pass<true>(H, 0ull, [&](int i) {
+            return crt_signed(untwist<LOGL, 0>(X[pad(i)], i, tw), untwist<LOGL, 1>(A1[pad(i)], i, tw), LOGH, cc,
+                              i == 0 ? OFF_N0 : OFF_C);
+        }, X, cs);
     } else {
-        for (int i = tid; i < H; i += T) sp.t[i] = X[pad(i)];
-        load_x(X, false);
+        // T = X: S = D = X
+        for (int i = tid; i < H; i += T) A0[pad(i)] = X[pad(i)];
+        __syncthreads();
     }
-    // m = T_lo * N' mod R
-    product_from<false, 0, LOGL, 1, false, true>(A, nullptr, tw, cd.nph, nullptr, cc);
-    spill_H();
-    load_x(sp.t, true);
-    product_from<false, 1, LOGL, 1, false, true>(A, nullptr, tw, cd.nph + L, nullptr, cc);
-    carry_pass<true>(
-        H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl, cc); }, A, cs);
-    for (int i = tid; i < H; i += T) sp.t[i] = A[pad(i)];
+    // m: D == X - cD (mod B^H + 1), cD < 2^39 folded into limbs 0 and 1
+    // (signed limbs, represented mod p)
+    unsigned long long cM;
+    {
+        const uint32_t c0 = (uint32_t)cD & LIMB_MASK, c1 = (uint32_t)(cD >> LIMB_BITS);
+        for (int i = tid; i < H; i += T) {
+            const uint32_t v = X[pad(i)], c = i == 0 ? c0 : (i == 1 ? c1 : 0u);
+            X[pad(i)] = twist<LOGL, 0>(v + P1 - c, i, tw);
+            A1[pad(i)] = twist<LOGL, 1>(v + P2 - c, i, tw);
+        }
+        __syncthreads();
+        product_from<true, 0, LOGH, 1, false>(X, A1, tw, cd.nn, cd.nn + H, cc);
+        cM = carry_pass<true>(H, 0ull, [&](int i) {
+            return crt_signed(untwist<LOGL, 0>(X[pad(i)], i, tw), untwist<LOGL, 1>(A1[pad(i)], i, tw), LOGH, cc,
+                              i == 0 ? OFF_N0 : OFF_C);
+        }, X, cs);
+    }
+    // m = lo - cM, plus R' when lo < cM (lo: the H limbs in X); modulo
+    // B^H - 1 that is lo - cM + 2 neg
+    bool z = true;
+    for (int i = tid; i < H; i += T) z = z && (i < 2 || X[pad(i)] == 0u);
+    const bool upper_zero = __syncthreads_and(z) != 0;
+    const bool neg = upper_zero && ((((unsigned long long)X[pad(1)] << LIMB_BITS) | X[pad(0)]) < cM);
     __syncthreads();
-    // W = m * N mod (R - 1)
-    product_from<false, 0, LOGL - 1, 1, false>(A, nullptr, tw, cd.nh, nullptr, cc);
-    spill_H();
-    for (int i = tid; i < H; i += T) A[pad(i)] = ldg_spill(sp.t + i);
-    __syncthreads();
-    product_from<false, 1, LOGL - 1, 1, false>(A, nullptr, tw, cd.nh + H, nullptr, cc);
-    const unsigned long long cW = carry_pass<true>(
-        H, 0ull, [&](int i) { return crt(ldg_spill(sp.s + spill_slot<H>(i)), A[pad(i)], logl - 1, cc); }, A, cs);
-    unsigned long long c = carry_pass<true>(
-        H, cS + cW, [&](int i) { return (unsigned long long)X[pad(i)] + A[pad(i)]; }, X, cs);
+    {
+        const uint32_t m0 = (uint32_t)cM & LIMB_MASK, m1 = (uint32_t)(cM >> LIMB_BITS);
+        for (int i = tid; i < H; i += T) {
+            const uint32_t v = X[pad(i)] + (i == 0 && neg ? 2u : 0u), c = i == 0 ? m0 : (i == 1 ? m1 : 0u);
+            X[pad(i)] = v + P1 - c;
+            A1[pad(i)] = v + P2 - c;
+        }
+        __syncthreads();
+    }
+    // W = m N (mod B^H - 1), then V = S + W into X; end-around carries
+    product_from<true, 0, LOGH, 1, false>(X, A1, tw, cd.nh, cd.nh + H, cc);
+    unsigned long long c = carry_pass<true>(H, cS, [&](int i) {
+        return (unsigned long long)A0[pad(i)] + crt_signed(X[pad(i)], A1[pad(i)], LOGH, cc, OFF_C);
+    }, X, cs);
     while (c) c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
-    if (a > 1u) carry_pass<true>(H, 0ull, [&](int i) { return (unsigned long long)X[pad(i)] * a; }, X, cs);
+    // V = B^H - 1 represents 0 (U = 0: T = 0)
+    bool ones = true;
+    for (int i = tid; i < H; i += T) ones = ones && (X[pad(i)] == LIMB_MASK);
+    if (__syncthreads_and(ones))
+        for (int i = tid; i < H; i += T) X[pad(i)] = 0u;
+    __syncthreads();
+    // X = a U from V = 2U
+    if (a & 1u) {
+        for (int i = tid; i < H; i += T) {
+            const uint32_t nx = X[pad(i + 1 < H ? i + 1 : 0)];
+            A1[pad(i)] = (X[pad(i)] >> 1) | ((nx & 1u) << (LIMB_BITS - 1));
+        }
+        __syncthreads();
+        if (a > 1u) {
+            carry_pass<true>(H, 0ull, [&](int i) { return (unsigned long long)A1[pad(i)] * a; }, X, cs);
+        } else {
+            for (int i = tid; i < H; i += T) X[pad(i)] = A1[pad(i)];
+            __syncthreads();
+        }
+    } else if (a > 2u) {
+        carry_pass<true>(H, 0ull, [&](int i) { return (unsigned long long)X[pad(i)] * (a >> 1); }, X, cs);
+    }
 }
 
 }  // namespace mr

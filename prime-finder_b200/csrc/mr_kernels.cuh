@@ -19,14 +19,12 @@ __constant__ CrtConsts c_crt;
 struct JobDev {
     uint32_t *x;          // H limbs: Montgomery residue (working value)
     uint32_t *res;        // H limbs: canonical residue a^E mod N (output)
-    uint32_t *nph;        // [2][L] NTT_L(N')
+    uint32_t *nn;         // [2][H] negacyclic NTT_H(N''), N'' = -N^-1 mod (B^H + 1)
     uint32_t *nh;         // [2][H] NTT_H(N)
-    const uint32_t *npl;  // H limbs of N' (set-up input)
+    const uint32_t *npl;  // H limbs of N'' (set-up input)
     const uint32_t *nl;   // H limbs of N
     const uint32_t *exp;  // exponent, 32-bit words, little-endian
-    uint32_t *spill_s;    // L words  (sequential-prime step only)
-    uint32_t *spill_t;    // H words  (sequential-prime step only)
-    uint32_t *ybuf;       // H words  (sequential-prime step only: canonical residue)
+    uint32_t *ybuf;       // H + H/32 words (L = 2^15 only: the residue Y, padded)
     struct LucasDev *lucas;  // strong Lucas test (mode 2) only
     int logl;
     int cursor;   // next exponent bit (MSB first); phase 0 while >= 0
@@ -46,31 +44,81 @@ struct LucasDev {
     uint32_t lb;  // every stored value is < lb * N
 };
 
-// Shared memory: both primes' transforms + X + Y up to L = 2^LOG_LCTA; one
-// transform + X above (the sequential-prime step keeps Y in global memory).
+// Shared memory: three transform buffers of H padded words (A0, A1, X) and,
+// up to L = 2^LOG_LCTA, a fourth for the residue Y (at L = 2^15, Y lives in
+// the candidate's global ybuf).
 __host__ __device__ inline size_t smem_words(int logl) {
-    const size_t L = (size_t)1 << logl, H = L / 2;
-    return logl <= LOG_LCTA ? 2 * (L + L / 32) + 2 * (H + H / 32) : (L + L / 32) + (H + H / 32);
+    const size_t H = (size_t)1 << (logl - 1), B = H + H / 32;
+    return (logl <= LOG_LCTA ? 4 : 3) * B;
 }
 inline size_t smem_bytes(int logl) {
     return smem_words(logl) * sizeof(uint32_t) + sizeof(CarrySmem) + 16;
 }
 
 __device__ __forceinline__ void carve(uint32_t *raw, int logl, Smem &sm, uint32_t *&Y, uint32_t *ybuf) {
-    const int L = 1 << logl, H = L >> 1;
+    const int H = 1 << (logl - 1), B = H + H / 32;
     sm.A0 = raw;
-    if (logl <= LOG_LCTA) {
-        sm.A1 = raw + L + L / 32;
-        sm.X = sm.A1 + L + L / 32;
-        Y = sm.X + H + H / 32;
-    } else {
-        sm.A1 = nullptr;
-        sm.X = raw + L + L / 32;
-        Y = ybuf;
-    }
+    sm.A1 = raw + B;
+    sm.X = raw + 2 * B;
+    Y = logl <= LOG_LCTA ? raw + 3 * B : ybuf;
     uintptr_t c = (uintptr_t)(raw + smem_words(logl));
     c = (c + 15) & ~(uintptr_t)15;
     sm.cs = (CarrySmem *)c;
+}
+
+// Cyclic (gc1, gc2: primes 1, 2) and negacyclic (gn1, gn2) NTT_H of the H
+// limbs at src, reduced (either pair may be null); uses A0 and A1.  Together
+// they are the two halves of the length-L transform of the zero-padded limbs.
+template <int LOGL>
+__device__ void spectra_t(const Smem &sm, const uint32_t *src, uint32_t *gc1, uint32_t *gc2, uint32_t *gn1,
+                          uint32_t *gn2, const Twiddles &tw, bool cg) {
+    constexpr int H = 1 << (LOGL - 1), LOGH = LOGL - 1;
+    const int tid = threadIdx.x;
+    for (int neg = 0; neg < 2; neg++) {
+        uint32_t *g1 = neg ? gn1 : gc1, *g2 = neg ? gn2 : gc2;
+        if (!g1) continue;
+        for (int i = tid; i < H; i += THREADS) {
+            const uint32_t v = cg ? __ldcg(src + i) : src[i];
+            sm.A0[pad(i)] = neg ? twist<LOGL, 0>(v, i, tw) : v;
+            sm.A1[pad(i)] = neg ? twist<LOGL, 1>(v, i, tw) : v;
+        }
+        __syncthreads();
+        dif_from<true, 0, LOGH, LOGH>(sm.A0, sm.A1, tw);
+        for (int i = tid; i < H; i += THREADS) {
+            g1[i] = red2(sm.A0[pad(i)], P1);
+            g2[i] = red2(sm.A1[pad(i)], P2);
+        }
+        __syncthreads();
+    }
+}
+
+#define PFB_LOGL_SWITCH(logl, CALL)                                   \
+    switch (logl) {                                                   \
+    case 8: { constexpr int LG = 8; CALL; } break;                    \
+    case 9: { constexpr int LG = 9; CALL; } break;                    \
+    case 10: { constexpr int LG = 10; CALL; } break;                  \
+    case 11: { constexpr int LG = 11; CALL; } break;                  \
+    case 12: { constexpr int LG = 12; CALL; } break;                  \
+    case 13: { constexpr int LG = 13; CALL; } break;                  \
+    case 14: { constexpr int LG = 14; CALL; } break;                  \
+    case 15: { constexpr int LG = 15; CALL; } break;                  \
+    }
+
+// g[2][L] <- the spectrum of a second factor for mont_step: per prime, the
+// cyclic half then the negacyclic half, of the H limbs at src, which may have
+// been written earlier in the same launch (L2-coherent loads).
+__device__ void spectrum(const Smem &sm, int logl, const uint32_t *src, uint32_t *g, const Twiddles &tw) {
+    const int L = 1 << logl, H = L >> 1;
+    PFB_LOGL_SWITCH(logl, (spectra_t<LG>(sm, src, g, g + L, g + H, g + L + H, tw, true)))
+}
+
+// Set-up of one candidate: the negacyclic spectrum of N'' (cd.nn) and the
+// cyclic spectrum of N (cd.nh), each [2][H].
+template <int LOGL>
+__device__ void prep_t(const Smem &sm, const JobDev &jb, const Twiddles &tw) {
+    constexpr int H = 1 << (LOGL - 1);
+    spectra_t<LOGL>(sm, jb.npl, nullptr, nullptr, jb.nn, jb.nn + H, tw, false);
+    spectra_t<LOGL>(sm, jb.nl, jb.nh, jb.nh + H, nullptr, nullptr, tw, false);
 }
 
 __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, const int *list, Twiddles tw) {
@@ -80,94 +128,52 @@ __global__ void __launch_bounds__(THREADS, 1) prep_kernel(JobDev *jobs, const in
     Smem sm;
     uint32_t *Y;
     carve(raw, jb.logl, sm, Y, jb.ybuf);
-    const int L = 1 << jb.logl, H = L >> 1;
-    if (jb.logl <= LOG_LCTA) {
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            const uint32_t v = i < H ? jb.npl[i] : 0u;
-            sm.A0[pad(i)] = v;
-            sm.A1[pad(i)] = v;
-        }
-        __syncthreads();
-        dif(sm.A0, sm.A1, jb.logl, tw);
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            jb.nph[i] = red2(sm.A0[pad(i)], P1);
-            jb.nph[L + i] = red2(sm.A1[pad(i)], P2);
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < H; i += blockDim.x) {
-            sm.A0[pad(i)] = jb.nl[i];
-            sm.A1[pad(i)] = jb.nl[i];
-        }
-        __syncthreads();
-        dif(sm.A0, sm.A1, jb.logl - 1, tw);
-        for (int i = threadIdx.x; i < H; i += blockDim.x) {
-            jb.nh[i] = red2(sm.A0[pad(i)], P1);
-            jb.nh[H + i] = red2(sm.A1[pad(i)], P2);
-        }
-        return;
-    }
-    uint32_t *A = sm.A0;
-    for (int pr = 0; pr < 2; pr++) {
-        for (int i = threadIdx.x; i < L; i += blockDim.x) A[pad(i)] = i < H ? jb.npl[i] : 0u;
-        __syncthreads();
-        if (pr == 0) dif1<0>(A, jb.logl, tw);
-        else dif1<1>(A, jb.logl, tw);
-        const uint32_t p = pr ? P2 : P1;
-        for (int i = threadIdx.x; i < L; i += blockDim.x) jb.nph[pr * L + i] = red2(A[pad(i)], p);
-        __syncthreads();
-        for (int i = threadIdx.x; i < H; i += blockDim.x) A[pad(i)] = jb.nl[i];
-        __syncthreads();
-        if (pr == 0) dif1<0>(A, jb.logl - 1, tw);
-        else dif1<1>(A, jb.logl - 1, tw);
-        for (int i = threadIdx.x; i < H; i += blockDim.x) jb.nh[pr * H + i] = red2(A[pad(i)], p);
-        __syncthreads();
-    }
+    PFB_LOGL_SWITCH(jb.logl, (prep_t<LG>(sm, jb, tw)))
 }
 
-// One Montgomery step in the layout chosen by the transform length (gy: the
-// spectrum of a second factor, see mont_step).
+// One Montgomery step at the candidate's transform length (gy: the spectrum
+// of a second factor, see mont_step).
 template <bool MUL>
 __device__ __forceinline__ void mstep_t(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                                        const JobDev &jb, const uint32_t *gy) {
-    static_assert(LOG_LCTA == 14 && LOG_LSEQ == 15, "length cases below");
-    switch (cd.logl) {
-#define PFB_STEP(n)                                                  \
-    case n:                                                          \
-        mont_step<MUL, n>(sm, cd, square, a, tw, c_crt, gy);        \
-        break;
-        PFB_STEP(8) PFB_STEP(9) PFB_STEP(10) PFB_STEP(11) PFB_STEP(12) PFB_STEP(13) PFB_STEP(14)
-#undef PFB_STEP
-    default: {
-        const Spill sp{jb.spill_s, jb.spill_t};
-        mont_step_seq<MUL, LOG_LSEQ>(sm, cd, square, a, tw, c_crt, sp, gy);
-    }
-    }
+                                        const uint32_t *gy) {
+    PFB_LOGL_SWITCH(cd.logl, (mont_step<MUL, LG>(sm, cd, square, a, tw, c_crt, gy)))
 }
 
 // The strong test's squarings (inlined into its loop).
 __device__ __forceinline__ void mstep(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                                      const JobDev &jb) {
-    mstep_t<false>(sm, cd, square, a, tw, jb, nullptr);
+                                      const JobDev &) {
+    mstep_t<false>(sm, cd, square, a, tw, nullptr);
 }
 
 // The Lucas ladder's steps: one out-of-line copy with the general product, so
 // the strong test's loop keeps its own register allocation.
 __device__ __noinline__ void mstep_l(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                                     const JobDev &jb, const uint32_t *gy) {
-    mstep_t<true>(sm, cd, square, a, tw, jb, gy);
+                                     const JobDev &, const uint32_t *gy) {
+    mstep_t<true>(sm, cd, square, a, tw, gy);
 }
 
-// Canonical residue of X (Montgomery form) into Y: Y = X R^-1 mod N.
+// Canonical residue of X (Montgomery form) into Y: Y = X R'^-1 mod N, X kept.
 template <bool LUCAS = false>
 __device__ void canonical(const Smem &sm, uint32_t *Y, const Cand &cd, const uint32_t *nl, const Twiddles &tw,
                           const JobDev &jb) {
     const int H = 1 << (cd.logl - 1);
     for (int i = threadIdx.x; i < H; i += blockDim.x) Y[pad(i)] = sm.X[pad(i)];
     __syncthreads();
-    Smem s2 = sm;
-    s2.X = Y;
-    if (LUCAS) mstep_l(s2, cd, false, 1u, tw, jb, nullptr);
-    else mstep(s2, cd, false, 1u, tw, jb);
+    if (cd.logl <= LOG_LCTA) {  // the step runs on Y in shared memory
+        Smem s2 = sm;
+        s2.X = Y;
+        if (LUCAS) mstep_l(s2, cd, false, 1u, tw, jb, nullptr);
+        else mstep(s2, cd, false, 1u, tw, jb);
+    } else {  // Y is in global memory: step on X, then exchange X and Y
+        if (LUCAS) mstep_l(sm, cd, false, 1u, tw, jb, nullptr);
+        else mstep(sm, cd, false, 1u, tw, jb);
+        for (int i = threadIdx.x; i < H; i += blockDim.x) {
+            const uint32_t t = sm.X[pad(i)];
+            sm.X[pad(i)] = Y[pad(i)];
+            Y[pad(i)] = t;
+        }
+        __syncthreads();
+    }
     // REDC(X) lies in [0, N]; it is N only when X == 0 (mod N), e.g. a base
     // that is a multiple of N.  Map it to 0.
     bool eqn = true;
@@ -196,36 +202,6 @@ __device__ __forceinline__ void load_res(uint32_t *X, const uint32_t *src, int H
 __device__ __forceinline__ void store_res(uint32_t *dst, const uint32_t *X, int H) {
     for (int i = threadIdx.x; i < H; i += blockDim.x) dst[i] = X[pad(i)];
     __syncthreads();
-}
-
-// g[2][L] <- NTT_L of the H limbs at src (zero-padded), both primes, reduced.
-__device__ void spectrum(const Smem &sm, int logl, const uint32_t *src, uint32_t *g, const Twiddles &tw) {
-    const int L = 1 << logl, H = L >> 1;
-    if (logl <= LOG_LCTA) {
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            const uint32_t v = i < H ? __ldcg(src + i) : 0u;
-            sm.A0[pad(i)] = v;
-            sm.A1[pad(i)] = v;
-        }
-        __syncthreads();
-        dif(sm.A0, sm.A1, logl, tw);
-        for (int i = threadIdx.x; i < L; i += blockDim.x) {
-            g[i] = red2(sm.A0[pad(i)], P1);
-            g[L + i] = red2(sm.A1[pad(i)], P2);
-        }
-        __syncthreads();
-        return;
-    }
-    uint32_t *A = sm.A0;
-    for (int pr = 0; pr < 2; pr++) {
-        for (int i = threadIdx.x; i < L; i += blockDim.x) A[pad(i)] = i < H ? __ldcg(src + i) : 0u;
-        __syncthreads();
-        if (pr == 0) dif1<0>(A, logl, tw);
-        else dif1<1>(A, logl, tw);
-        const uint32_t p = pr ? P2 : P1;
-        for (int i = threadIdx.x; i < L; i += blockDim.x) g[pr * L + i] = red2(A[pad(i)], p);
-        __syncthreads();
-    }
 }
 
 // out <- x + c y (sub = false) or x + c (m N - y) (sub = true: x - c y mod N,
@@ -294,7 +270,7 @@ __device__ void lucas_bit(const Smem &sm, const Cand &cd, const JobDev &jb, cons
 // Strong Lucas steps of one candidate (mode 2); returns steps taken.
 __device__ __noinline__ int run_lucas(JobDev &jb, const Smem &sm, uint32_t *Y, int max_steps, const Twiddles &tw, int &cursor,
                          int &phase, int &extra, int &verdict) {
-    const Cand cd{jb.nph, jb.nh, jb.logl};
+    const Cand cd{jb.nn, jb.nh, jb.logl};
     const LucasDev lc = *jb.lucas;
     const int H = 1 << (jb.logl - 1);
     CarrySmem &cs = *sm.cs;
@@ -366,7 +342,7 @@ __device__ void run_job(JobDev *jp, int max_steps, const Twiddles &tw, uint32_t 
     uint32_t *Y;
     carve(raw, jb.logl, sm, Y, jb.ybuf);
     const int H = 1 << (jb.logl - 1);
-    const Cand cd{jb.nph, jb.nh, jb.logl};
+    const Cand cd{jb.nn, jb.nh, jb.logl};
     int cursor = jb.cursor, phase = jb.phase, extra = jb.extra, verdict = jb.verdict, steps = 0;
     if (jb.mode == 2) {
         steps = run_lucas(jb, sm, Y, max_steps, tw, cursor, phase, extra, verdict);

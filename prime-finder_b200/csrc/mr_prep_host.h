@@ -1,7 +1,9 @@
-// Host set-up of one candidate for the Miller-Rabin engine (N' by Hensel
-// lifting, R mod N, the exponent and its bit cursor; for the strong Lucas
-// test Selfridge's parameters and V_0 = 2 in Montgomery form): the job GMP
-// does in the reference (barrett.cu:58-107, montgomery.cu:30-45).
+// Host set-up of one candidate for the Miller-Rabin engine (the Montgomery
+// radix R' = 2^(22 H) + 1 of the transform length, N'' = -N^-1 mod R' by
+// Lehmer's extended Euclid, R' mod N, the exponent and its bit cursor; for
+// the strong Lucas test Selfridge's parameters and V_0 = 2 in Montgomery
+// form): the job GMP does in the reference (barrett.cu:58-107,
+// montgomery.cu:30-45).
 #pragma once
 #include <stdint.h>
 
@@ -20,7 +22,7 @@ struct HostPrep {
     int decided = -1;  // >= 0: verdict known without device work (Lucas: a factor, a square)
     int logl = 0;
     int s = 0;
-    std::vector<uint32_t> x0, npl, nl, exp;
+    std::vector<uint32_t> x0, npl, nl, exp;  // R' mod N, N'', N (H limbs each), exponent words
     int cursor = 0;
     int n16 = 0;  // limbs of N (16-bit)
     int q = 0;                 // Lucas: Q
@@ -61,8 +63,23 @@ inline void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const
         hp.lb = 2u + 4u * aq * aq;
         base = hp.lb;
     }
-    const int lg = choose_logl(nb, base);
+    int lg = choose_logl(nb, base);
     if (lg < 0) return;
+    // N'' = -N^-1 mod R'; when N shares a factor with R' = 2^(22 H) + 1
+    // (possible for a prime factor of such a number), the next length's
+    // R'' = R'^2 - 2 R' + 2 shares none of them
+    Words inv;
+    for (; lg <= LOG_LSEQ; lg++) {
+        const size_t rb = (size_t)LIMB_BITS << (lg - 1);
+        Words M(rb / 64 + 1, 0);
+        M[rb / 64] = 1ull << (rb % 64);
+        M[0] |= 1ull;
+        if (inv_mod(N, M, &inv)) {
+            inv = sub(M, inv);
+            break;
+        }
+    }
+    if (lg > LOG_LSEQ) return;
     const size_t H = (size_t)1 << (lg - 1);
     const size_t rbits = LIMB_BITS * H;
     Words E;
@@ -89,9 +106,10 @@ inline void host_prep(const pfb_mr_number_t &num, uint32_t base, int mode, const
     hp.npl.assign(H, 0);
     hp.nl.assign(H, 0);
     hp.x0.assign(H, 0);
-    to_limbs(neg_inv_pow2(N, rbits), LIMB_BITS, hp.npl.data(), H);
+    to_limbs(inv, LIMB_BITS, hp.npl.data(), H);
     to_limbs(N, LIMB_BITS, hp.nl.data(), H);
-    const Words x0 = pow2_mod(rbits, N);
+    Words x0 = add(pow2_mod(rbits, N), Words(1, 1));  // R' mod N
+    if (cmp(x0, N) >= 0) x0 = sub(x0, N);
     to_limbs(x0, LIMB_BITS, hp.x0.data(), H);
     if (mode == 2) {
         hp.v0.assign(H, 0);

@@ -5,6 +5,7 @@
 //   divmod U V        -> quotient remainder
 //   pow2_mod e N      -> 2^e mod N              (e decimal)
 //   neg_inv N bits    -> -N^-1 mod 2^bits       (bits decimal)
+//   inv_mod A M       -> A^-1 mod M, or "-" when gcd(A, M) != 1
 //   mul A B / sub A B / shl A s / shr A s / isqrt A / pow10 e / mod_small A m
 //   limbs A bits n    -> from_limbs(to_limbs(A)) (round trip through n limbs)
 //   u16 A n           -> from_u16(to_u16(A))     (round trip through n limbs)
@@ -63,6 +64,9 @@ int main() {
             std::cout << to_hex(pow2_mod(std::stoull(x), from_hex(y))) << "\n";
         } else if (op == "neg_inv") {
             std::cout << to_hex(neg_inv_pow2(from_hex(x), std::stoull(y))) << "\n";
+        } else if (op == "inv_mod") {
+            Words r;
+            std::cout << (inv_mod(from_hex(x), from_hex(y), &r) ? to_hex(r) : std::string("-")) << "\n";
         } else if (op == "mul") {
             std::cout << to_hex(mul(from_hex(x), from_hex(y))) << "\n";
         } else if (op == "sub") {

@@ -88,23 +88,20 @@ int main() {
             continue;
         }
         const int L = 1 << hp.logl, H = L >> 1;
-        std::vector<uint32_t> x(H), res(H), nph(2 * L), nh(2 * H), npl = hp.npl, nl = hp.nl;
-        std::vector<uint32_t> ss(L), st(H), yb(H + H / 32), gy(2 * L), yl(H);
+        std::vector<uint32_t> x(H), res(H), nn(2 * H), nh(2 * H), npl = hp.npl, nl = hp.nl;
+        std::vector<uint32_t> yb(H + H / 32), gy(2 * L), yl(H);
+        std::vector<unsigned long long> rawc(L);
         JobDev j{};
         j.x = x.data();
         j.res = res.data();
-        j.nph = nph.data();
+        j.nn = nn.data();
         j.nh = nh.data();
         j.npl = npl.data();
         j.nl = nl.data();
-        if (hp.logl > LOG_LCTA) {
-            j.spill_s = ss.data();
-            j.spill_t = st.data();
-            j.ybuf = yb.data();
-        }
+        if (hp.logl > LOG_LCTA) j.ybuf = yb.data();
         j.logl = hp.logl;
         j.phase = 0;
-        CtxExtra ex{gy.data(), yl.data()};
+        CtxExtra ex{gy.data(), yl.data(), rawc.data()};
         const size_t smem = smem_bytes(hp.logl);
         emu::run_grid(1, 1, THREADS, [&] { prep_kernel(&j, nullptr, tw); }, smem);
         const std::vector<uint64_t> A = limbs64(from_hex(sa), n16), B = limbs64(from_hex(sb), n16);

@@ -1,16 +1,15 @@
-// Runs the engine's Montgomery step (mr_device.cuh: mont_step, and
-// mont_step_seq for L = 2^15) unchanged on the CPU: one CTA of THREADS
-// cooperative fibers (tests/cpp/emul/cuda_runtime.h), with the engine's own constant
-// tables (mr_tables_host.h) and set-up (bigint_host.h).  Each input line is
+// Runs the engine's Montgomery step (mr_device.cuh: mont_step, the radix
+// R' = 2^(22 H) + 1) unchanged on the CPU: one CTA of THREADS cooperative
+// fibers (tests/cpp/emul/cuda_runtime.h), with the engine's own constant
+// tables (mr_tables_host.h), set-up of N'' (bigint_host.h: inv_mod) and
+// spectra (mr_kernels.cuh: spectra_t, spectrum).  Each input line is
 //
 //   step logl N x a      -> X <- REDC(x^2) * a
 //   mul  logl N x y a    -> X <- REDC(x y) * a   (y through its stored spectrum)
 //   redc logl N x        -> X <- REDC(x)
 //
-// with N, x, y in hexadecimal; the output line is X in hexadecimal.  The
-// device set-up (NTT of N' and of N, the spectrum of y) follows mr.cu's
-// prep_kernel and spectrum for the lengths whose two primes share the CTA,
-// and their one-prime-at-a-time form at L = 2^15.
+// with N, x, y in hexadecimal; the output line is X in hexadecimal.  Every
+// buffer is a host array of exactly the size the kernel's layout gives it.
 #include <functional>
 #include <iostream>
 #include <sstream>
@@ -18,7 +17,7 @@
 #include <vector>
 
 #include "bigint_host.h"
-#include "mr_device.cuh"
+#include "mr_kernels.cuh"
 #include "mr_tables_host.h"
 
 using namespace pfb::mr;
@@ -76,44 +75,14 @@ struct Tables {
 
 template <bool MUL>
 static void step_len(int logl, const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
-                     const CrtConsts &cc, const Spill &sp, const uint32_t *gy) {
+                     const CrtConsts &cc, const uint32_t *gy) {
     switch (logl) {
         case 8: mont_step<MUL, 8>(sm, cd, square, a, tw, cc, gy); break;
         case 9: mont_step<MUL, 9>(sm, cd, square, a, tw, cc, gy); break;
         case 10: mont_step<MUL, 10>(sm, cd, square, a, tw, cc, gy); break;
         case 14: mont_step<MUL, 14>(sm, cd, square, a, tw, cc, gy); break;
-        case 15: mont_step_seq<MUL, 15>(sm, cd, square, a, tw, cc, sp, gy); break;
+        case 15: mont_step<MUL, 15>(sm, cd, square, a, tw, cc, gy); break;
         default: break;
-    }
-}
-
-// NTT_n of the zero-padded limbs src (m of them) into g[2][n], both primes, reduced.
-static void spectrum(uint32_t *A0, uint32_t *A1, int logn, const uint32_t *src, int m, uint32_t *g,
-                     const Twiddles &tw) {
-    const int n = 1 << logn, T = (int)blockDim.x, tid = (int)threadIdx.x;
-    if (A1) {
-        for (int i = tid; i < n; i += T) {
-            const uint32_t v = i < m ? src[i] : 0u;
-            A0[pad(i)] = v;
-            A1[pad(i)] = v;
-        }
-        __syncthreads();
-        dif(A0, A1, logn, tw);
-        for (int i = tid; i < n; i += T) {
-            g[i] = red2(A0[pad(i)], P1);
-            g[n + i] = red2(A1[pad(i)], P2);
-        }
-        __syncthreads();
-        return;
-    }
-    for (int pr = 0; pr < 2; pr++) {
-        for (int i = tid; i < n; i += T) A0[pad(i)] = i < m ? src[i] : 0u;
-        __syncthreads();
-        if (pr == 0) dif1<0>(A0, logn, tw);
-        else dif1<1>(A0, logn, tw);
-        const uint32_t p = pr ? P2 : P1;
-        for (int i = tid; i < n; i += T) g[pr * n + i] = red2(A0[pad(i)], p);
-        __syncthreads();
     }
 }
 
@@ -134,30 +103,49 @@ int main() {
             in >> a;
         }
         const int L = 1 << logl, H = L >> 1;
-        const bool seq = logl > LOG_LCTA;
         const Words N = from_hex(sn), x = from_hex(sx);
+        // N'' = -N^-1 mod (2^(22 H) + 1)
+        const size_t rb = (size_t)LIMB_BITS * H;
+        Words M(rb / 64 + 1, 0), inv;
+        M[rb / 64] = 1ull << (rb % 64);
+        M[0] |= 1ull;
+        if (!pfb::big::inv_mod(N, M, &inv)) {
+            std::cout << "-" << std::endl;
+            continue;
+        }
+        inv = pfb::big::sub(M, inv);
         std::vector<uint32_t> npl(H), nl(H), xl(H), yl(H);
-        pfb::big::to_limbs(pfb::big::neg_inv_pow2(N, (size_t)LIMB_BITS * H), LIMB_BITS, npl.data(), H);
+        pfb::big::to_limbs(inv, LIMB_BITS, npl.data(), H);
         pfb::big::to_limbs(N, LIMB_BITS, nl.data(), H);
         pfb::big::to_limbs(x, LIMB_BITS, xl.data(), H);
         pfb::big::to_limbs(Y, LIMB_BITS, yl.data(), H);
-        std::vector<uint32_t> A0(L + L / 32), A1(seq ? 0 : L + L / 32), X(H + H / 32);
-        std::vector<uint32_t> nph(2 * L), nh(2 * H), gy(2 * L), ss(L + H + H / 32), st(H);
+        const int B = H + H / 32;
+        std::vector<uint32_t> A0(B), A1(B), X(B);
+        std::vector<uint32_t> nn(2 * H), nh(2 * H), gy(2 * L);
         CarrySmem cs{};
-        uint32_t *a1 = seq ? nullptr : A1.data();
-        const Smem sm{A0.data(), a1, X.data(), &cs};
-        const Cand cd{nph.data(), nh.data(), logl};
-        const Spill sp{ss.data(), st.data()};
+        const Smem sm{A0.data(), A1.data(), X.data(), &cs};
+        const Cand cd{nn.data(), nh.data(), logl};
         run_cta([&] {
-            spectrum(A0.data(), a1, logl, npl.data(), H, nph.data(), tb.tw);
-            spectrum(A0.data(), a1, logl - 1, nl.data(), H, nh.data(), tb.tw);
-            if (op == "mul") spectrum(A0.data(), a1, logl, yl.data(), H, gy.data(), tb.tw);
+            switch (logl) {
+                case 8: spectra_t<8>(sm, npl.data(), nullptr, nullptr, nn.data(), nn.data() + H, tb.tw, false); break;
+                case 9: spectra_t<9>(sm, npl.data(), nullptr, nullptr, nn.data(), nn.data() + H, tb.tw, false); break;
+                case 10: spectra_t<10>(sm, npl.data(), nullptr, nullptr, nn.data(), nn.data() + H, tb.tw, false); break;
+                case 14: spectra_t<14>(sm, npl.data(), nullptr, nullptr, nn.data(), nn.data() + H, tb.tw, false); break;
+                case 15: spectra_t<15>(sm, npl.data(), nullptr, nullptr, nn.data(), nn.data() + H, tb.tw, false); break;
+            }
+            spectrum(sm, logl, nl.data(), gy.data(), tb.tw);  // cyclic half of N: gy[0..H), gy[L..L+H)
+            for (int i = (int)threadIdx.x; i < H; i += (int)blockDim.x) {
+                nh[i] = gy[i];
+                nh[H + i] = gy[L + i];
+            }
+            __syncthreads();
+            if (op == "mul") spectrum(sm, logl, yl.data(), gy.data(), tb.tw);
             for (int i = (int)threadIdx.x; i < H; i += (int)blockDim.x) X[pad(i)] = xl[i];
             __syncthreads();
             if (op == "mul")
-                step_len<true>(logl, sm, cd, false, a, tb.tw, tb.cc, sp, gy.data());
+                step_len<true>(logl, sm, cd, false, a, tb.tw, tb.cc, gy.data());
             else
-                step_len<false>(logl, sm, cd, op == "step", a, tb.tw, tb.cc, sp, nullptr);
+                step_len<false>(logl, sm, cd, op == "step", a, tb.tw, tb.cc, nullptr);
         });
         std::vector<uint32_t> out(H);
         for (int i = 0; i < H; i++) out[i] = X[i + (i >> 5)];

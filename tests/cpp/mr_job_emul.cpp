@@ -84,22 +84,18 @@ int main() {
             continue;
         }
         const int L = 1 << hp.logl, H = L >> 1;
-        std::vector<uint32_t> x = hp.x0, res(H), nph(2 * L), nh(2 * H), npl = hp.npl, nl = hp.nl, ex = hp.exp;
-        std::vector<uint32_t> ss(L), st(H), yb(H + H / 32);
+        std::vector<uint32_t> x = hp.x0, res(H), nn(2 * H), nh(2 * H), npl = hp.npl, nl = hp.nl, ex = hp.exp;
+        std::vector<uint32_t> yb(H + H / 32);
         std::vector<uint32_t> lv0 = hp.v0, lv1 = hp.x0, lqk = hp.x0, lone = hp.x0, lt(H), gy(2 * L);
         JobDev j{};
         j.x = x.data();
         j.res = res.data();
-        j.nph = nph.data();
+        j.nn = nn.data();
         j.nh = nh.data();
         j.npl = npl.data();
         j.nl = nl.data();
         j.exp = ex.data();
-        if (hp.logl > LOG_LCTA) {
-            j.spill_s = ss.data();
-            j.spill_t = st.data();
-            j.ybuf = yb.data();
-        }
+        if (hp.logl > LOG_LCTA) j.ybuf = yb.data();
         j.logl = hp.logl;
         j.cursor = hp.cursor;
         j.extra = mode >= 1 ? hp.s - 1 : 0;

@@ -181,3 +181,36 @@ def test_selfridge_parameters(run):
     for n, line in zip(ns, out):
         want = lucas.selfridge_d(n)
         assert line == ("0" if want is None else "1 %d" % want), n
+
+
+def test_inv_mod_lehmer(run):
+    """Lehmer's extended Euclid (inv_mod): the inverse of N modulo
+    2^(22 H) + 1, the Montgomery radix of the engine, for moduli of every
+    transform length up to 100 000 digits, random odd moduli, and pairs with a
+    common factor (no inverse)."""
+    rng = random.Random(77)
+    cases = []
+    for H in (128, 1024, 8192, 16384):
+        M = (1 << (22 * H)) + 1
+        for bits in (20, 100, 22 * H - 40, 22 * H - 6):
+            a = rng.getrandbits(bits) | (1 << (bits - 1)) | 1
+            cases.append((a, M))
+    for _ in range(40):
+        M = rng.getrandbits(rng.choice([65, 128, 700, 3000])) | 1
+        a = rng.randrange(1, M)
+        cases.append((a, M))
+    cases += [(3, 7), (1, 5), (6, 9), (10, 25), ((1 << 200) + 1, (1 << 400) - 1)]
+    # a prime factor of the Fermat number 2^256 + 1 divides 2^(22*128) + 1
+    cases.append((1238926361552897, (1 << 2816) + 1))
+    # moduli of the Montgomery-step tests (one of them once met a Lehmer step
+    # whose single-precision matrix had A = 0)
+    r2 = random.Random(115)
+    for abits in (1, 2, 2, 17):
+        nb = 22 * 16384 - 2 - 2 * abits - r2.randrange(0, 60)
+        cases.append((r2.getrandbits(nb) | 1 | (1 << (nb - 1)), (1 << (22 * 16384)) + 1))
+    out = run(["inv_mod %s %s" % (h(a), h(M)) for a, M in cases])
+    for (a, M), got in zip(cases, out):
+        if math.gcd(a, M) != 1:
+            assert got == "-", (a, M)
+        else:
+            assert int(got, 16) == pow(a, -1, M), (a.bit_length(), M.bit_length())

@@ -3,11 +3,12 @@
 tests/cpp/ctx_emul.cpp drives the engine's host set-up, its set-up kernel
 and the context's operation kernel (csrc/mr_ctx_kernels.cuh: ctx_kernel)
 unchanged through the stand-in CUDA runtime of tests/cpp/emul/, one modulus
-per CTA.  With R = 2^(22 H) of the modulus' transform length, every result
-must equal Python's integers: REDC(a^2) and REDC(a b) = a b R^-1 mod N fully
-reduced, the raw products a^2 and a b over n_sum = 2 n16 + 16 limbs, and
-a R^-1 mod N; at transform lengths 2^8 to 2^15 (the longest one spills a
-prime's coefficients to global memory), and once under AddressSanitizer.
+per CTA.  With R' = 2^(22 H) + 1 of the modulus' transform length, every
+result must equal Python's integers: REDC(a^2) and REDC(a b) = a b R'^-1 mod N
+fully reduced, the raw products a^2 and a b over n_sum = 2 n16 + 16 limbs, and
+a R'^-1 mod N; at transform lengths 2^8 to 2^15 (the longest one keeps its
+residue conversion's output in global memory), and once under
+AddressSanitizer.
 """
 import os
 import random
@@ -59,7 +60,7 @@ def _cases(rng, bits_list):
 
 
 def _want(op, n16, N, a, b, logl):
-    R = 1 << (22 * (1 << (logl - 1)))
+    R = (1 << (22 * (1 << (logl - 1)))) + 1
     ri = pow(R, -1, N)
     if op == 0:
         return a * a * ri % N

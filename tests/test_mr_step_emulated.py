@@ -5,16 +5,18 @@ for the host against a stand-in for the CUDA runtime (tests/cpp/emul/): one
 CTA is THREADS cooperative fibers, __syncthreads a barrier over them, and the
 warp ballots and shuffles exchange values through a barrier over each warp.  The
 engine's own table builders (mr_tables_host.h) and modulus set-up
-(bigint_host.h) feed it.  Each result must equal, limb for limb, Montgomery's
-REDC as the kernel defines it: with R = 2^(22 H), N' = -N^-1 mod R,
-m = (T mod R) N' mod R and U = (T + m N) / R, the step leaves U * a for
-T = x^2 (squaring), T = x y (general product through y's stored spectrum,
-the Lucas test's form) or T = x (conversion out of Montgomery form).
+(bigint_host.h: N'' by Lehmer's extended Euclid) feed it.  Each result must
+equal, limb for limb, Montgomery's REDC as the kernel defines it: with the
+radix R' = 2^(22 H) + 1, m = -T N^-1 mod R' in [0, R') and
+U = (T + m N) / R', the step leaves U * a for T = x^2 (squaring), T = x y
+(general product through y's stored spectrum, the Lucas test's form) or
+T = x (conversion out of Montgomery form).
 
-This pins the arithmetic of the transforms, the fused pointwise sweep, the
-zero-padded first pass, the CRT, the carry-lookahead passes and the
-end-around carry at the transform lengths 2^8, 2^9, 2^10, 2^14 (both primes
-in one CTA) and 2^15 (one prime after the other, through the spill buffer).
+This pins the arithmetic of the cyclic and negacyclic transforms (the twist
+by a 2H-th root of unity), the fused pointwise sweep, the signed CRT with its
+offsets, the carry-lookahead passes, the end-around carry and the halving
+of V = 2U at the transform lengths 2^8, 2^9, 2^10, 2^14 and 2^15 (every
+length keeps both primes in one CTA).
 It does not stand in for the GPU tests: timing, memory ordering between
 CTAs and the scheduler are not emulated.
 """
@@ -47,20 +49,10 @@ def emul(tmp_path_factory):
     return run
 
 
-def neg_inv_pow2(N, k):
-    """-N^-1 mod 2^k for odd N (Newton: x <- x (2 - N x), doubling the bits)."""
-    x, bits = 1, 1
-    while bits < k:
-        bits = min(2 * bits, k)
-        x = (x * (2 - N * x)) & ((1 << bits) - 1)
-    return (-x) & ((1 << k) - 1)
-
-
 def redc(logl, N, T, a=1):
-    k = 22 << (logl - 1)  # R = 2^k: reductions by R are masks and shifts
-    mask = (1 << k) - 1
-    m = ((T & mask) * neg_inv_pow2(N, k)) & mask
-    return ((T + m * N) >> k) * a
+    R = (1 << (22 << (logl - 1))) + 1  # R' = 2^(22 H) + 1
+    m = (-T * pow(N, -1, R)) % R
+    return (T + m * N) // R * a
 
 
 def modulus(rng, logl, abits):
@@ -99,12 +91,12 @@ def test_general_product_and_conversion(emul, logl):
 def test_montgomery_ladder_equals_pow(emul):
     """A short square-and-multiply ladder in Montgomery form, fed back through
     the emulated step, ends at pow(2, e, N): the step composes as the
-    persistent kernel composes it (x0 = R mod N, one step per exponent bit,
+    persistent kernel composes it (x0 = R' mod N, one step per exponent bit,
     a final conversion)."""
     rng = random.Random(7)
     logl = 9
     H = 1 << (logl - 1)
-    R = 1 << (22 * H)
+    R = (1 << (22 * H)) + 1
     N = modulus(rng, logl, 2)
     e = rng.getrandbits(12) | (1 << 11)
     x = R % N
