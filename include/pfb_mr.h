@@ -130,9 +130,11 @@ void pfb_mr_batch_destroy(pfb_mr_batch_t *b);
  *   modsq/modmul  d_out = working form of a^2 / a b, from working forms
  *   sq_raw/mul_raw  d_out = the full product, n_sum = 2 n_limbs + 16 limbs
  *                 per modulus (the reference's n_sum), no reduction
- * Device pointers; each call is asynchronous on `stream` (NULL = the
- * engine's stream).  A context's scratch is shared by its calls: calls on one
- * context must not overlap on the GPU.
+ * Device pointers; each call is asynchronous on `stream` (NULL = the legacy
+ * default stream, where the reference's methods run, so that the caller's
+ * cudaMemcpy calls are ordered with them); from_residue runs on the default
+ * stream and returns when its result is on the host.  A context's scratch is
+ * shared by its calls: calls on one context must not overlap on the GPU.
  */
 typedef struct pfb_mr_ctx pfb_mr_ctx_t;
 int pfb_mr_ctx_create(pfb_mr_t *e, const uint64_t *N_all, int n_limbs, int n_batch, pfb_mr_ctx_t **out);
@@ -195,6 +197,13 @@ int pfb_mr_server_submit(pfb_mr_server_t *s, const uint16_t *limbs, int n_limbs,
  * number, or a negative PFB_E* code if the server stopped on an error. */
 int pfb_mr_server_poll(pfb_mr_server_t *s, pfb_mr_result_t *out, int cap, int timeout_ms);
 int pfb_mr_server_stats(pfb_mr_server_t *s, pfb_mr_server_stats_t *st);
+/* Test hook (host-side fault injection; nothing faults on the device): the
+ * next n allocations of slot memory fail as if cudaMalloc had returned
+ * cudaErrorMemoryAllocation, exercising the server's recovery (free the
+ * pooled blocks and retry; then requeue the request while others are
+ * resident, or fail it with verdict -1 when none is).  Returns the number of
+ * injected failures consumed so far. */
+int pfb_mr_server_inject_alloc_failures(pfb_mr_server_t *s, int n);
 /* Stops the loop (pending requests are dropped) and frees everything. */
 void pfb_mr_server_destroy(pfb_mr_server_t *s);
 

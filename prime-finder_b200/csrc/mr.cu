@@ -733,6 +733,9 @@ struct pfb_mr_server {
     std::vector<std::thread> workers;
     std::thread driver;
     int error = PFB_OK;
+    // host-side fault injection (pfb_mr_server_inject_alloc_failures)
+    int inject_alloc_failures = 0;
+    int injected_alloc_failures = 0;
 };
 
 namespace {
@@ -742,6 +745,20 @@ double now_s(const pfb_mr_server *s) {
 }
 
 size_t slot_bytes(int logl) { return slot_layout(logl).total * sizeof(uint32_t); }
+
+// Slot memory; a failure injected from the host (a test hook) is reported as
+// cudaErrorMemoryAllocation without calling cudaMalloc.
+cudaError_t srv_alloc(pfb_mr_server *s, uint8_t **mem, size_t need) {
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->inject_alloc_failures > 0) {
+            s->inject_alloc_failures--;
+            s->injected_alloc_failures++;
+            return cudaErrorMemoryAllocation;
+        }
+    }
+    return cudaMalloc(mem, need);
+}
 
 void srv_prep_worker(pfb_mr_server *s) {
     for (;;) {
@@ -841,7 +858,7 @@ int srv_admit(pfb_mr_server *s, std::vector<int> &admitted) {
         SrvSlot &sl = s->slots[admitted.back()];
         if (!sl.mem) {
             const size_t need = slot_bytes(sl.logl);
-            cudaError_t ce = cudaMalloc(&sl.mem, need);
+            cudaError_t ce = srv_alloc(s, &sl.mem, need);
             if (ce != cudaSuccess) {
                 // the device ran out below the budget (memory held elsewhere):
                 // give back the pooled blocks and try once more
@@ -856,8 +873,8 @@ int srv_admit(pfb_mr_server *s, std::vector<int> &admitted) {
                     kv.second.clear();
                 }
                 sl.mem = nullptr;
-                ce = cudaMalloc(&sl.mem, need);
             }
+            if (ce != cudaSuccess) ce = srv_alloc(s, &sl.mem, need);
             if (ce != cudaSuccess) {
                 // undo the admission: the request waits for resident candidates
                 // to retire, or fails if none is resident
@@ -1111,6 +1128,16 @@ extern "C" int pfb_mr_server_poll(pfb_mr_server_t *s, pfb_mr_result_t *out, int 
     return n;
 }
 
+extern "C" int pfb_mr_server_inject_alloc_failures(pfb_mr_server_t *s, int n) {
+    if (!s || n < 0) {
+        pfb::set_error("pfb_mr_server_inject_alloc_failures: bad argument");
+        return PFB_E_ARG;
+    }
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->inject_alloc_failures += n;
+    return s->injected_alloc_failures;
+}
+
 extern "C" int pfb_mr_server_stats(pfb_mr_server_t *s, pfb_mr_server_stats_t *st) {
     if (!s || !st) {
         pfb::set_error("pfb_mr_server_stats: bad argument");
@@ -1188,7 +1215,9 @@ int ctx_launch(pfb_mr_ctx *c, const uint64_t *a, const uint64_t *b, uint64_t *ou
         return PFB_E_ARG;
     }
     PFB_CUDA(cudaSetDevice(c->e->device));
-    cudaStream_t st = stream ? (cudaStream_t)stream : c->e->stream;
+    // NULL: the legacy default stream, ordered with the caller's other
+    // default-stream work (the reference's methods run there)
+    cudaStream_t st = stream ? (cudaStream_t)stream : cudaStreamLegacy;
     ctx_kernel<<<c->n, THREADS, smem_bytes(c->maxlog), st>>>(c->d_jobs, c->d_ex, a, b ? b : a, out, c->n16,
                                                               out_stride, op, c->e->tw);
     PFB_CUDA(cudaGetLastError());
@@ -1343,8 +1372,7 @@ extern "C" int pfb_mr_ctx_from_residue(pfb_mr_ctx_t *c, const uint64_t *d_x, uin
     }
     const int rc = ctx_launch(c, d_x, nullptr, c ? c->d_tmp : nullptr, c ? c->n16 : 0, CTX_FROM, nullptr);
     if (rc) return rc;
-    PFB_CUDA(cudaMemcpyAsync(out_all, c->d_tmp, (size_t)c->n * c->n16 * 8, cudaMemcpyDeviceToHost, c->e->stream));
-    PFB_CUDA(cudaStreamSynchronize(c->e->stream));
+    PFB_CUDA(cudaMemcpy(out_all, c->d_tmp, (size_t)c->n * c->n16 * 8, cudaMemcpyDeviceToHost));
     return PFB_OK;
 }
 
@@ -1354,7 +1382,7 @@ extern "C" int pfb_mr_ctx_check_passed(pfb_mr_ctx_t *c, const uint64_t *d_r, uin
         return PFB_E_ARG;
     }
     PFB_CUDA(cudaSetDevice(c->e->device));
-    cudaStream_t st = stream ? (cudaStream_t)stream : c->e->stream;
+    cudaStream_t st = stream ? (cudaStream_t)stream : cudaStreamLegacy;
     ctx_check_kernel<<<c->n, 256, 0, st>>>(d_r, c->d_one, c->d_nm1, d_passed, c->n16);
     PFB_CUDA(cudaGetLastError());
     return PFB_OK;

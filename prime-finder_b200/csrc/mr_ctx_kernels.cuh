@@ -71,38 +71,37 @@ __device__ __forceinline__ void cond_sub_n(uint32_t *X, uint32_t *T, const uint3
 }
 
 // The full product X Y (gy: the spectrum of Y) or X^2 of the H limbs in
-// sm.X, as L limbs of 22 bits in A0..A1 read as one padded array of L words
-// (A1 follows A0); no reduction.  With T(z) = A(z) + z^H C(z) the cyclic
-// product gives c = A + C and the negacyclic one d = A - C, coefficient by
-// coefficient, so T's coefficients are (c + d) / 2 and (c - d) / 2, both
-// exact; raw holds the 2H coefficients between the products and the carry.
+// sm.X, as L limbs of 22 bits in A0 read as one padded array of L words
+// (up to L = 2^LOG_LCTA A0 holds them; above, A1 follows A0); no reduction.
+// With T(z) = A(z) + z^H C(z) the cyclic product of length H gives c = A + C
+// and the negacyclic one d = A - C, coefficient by coefficient, so T's
+// coefficients are (c + d) / 2 and (c - d) / 2, both exact; raw holds the 2H
+// coefficients between the products and the carry.
 template <int LOGL>
 __device__ void raw_product_t(const Smem &sm, bool square, const uint32_t *gy, unsigned long long *raw,
                               const Twiddles &tw) {
     constexpr int L = 1 << LOGL, H = L >> 1, LOGH = LOGL - 1;
     const int tid = threadIdx.x;
     uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
-    for (int i = tid; i < H; i += THREADS) {
-        const uint32_t v = X[pad(i)];
-        A0[pad(i)] = v;
-        A1[pad(i)] = v;
+    for (int neg = 0; neg < 2; neg++) {
+        for (int i = tid; i < H; i += THREADS) {
+            const uint32_t v = X[pad(i)];
+            A0[pad(i)] = v;
+            A1[pad(i)] = v;
+        }
+        __syncthreads();
+        if (!neg) {
+            if (square) product_from<true, 0, LOGH, 0, false>(A0, A1, tw, nullptr, nullptr, c_crt);
+            else product_from<true, 0, LOGH, 1, true>(A0, A1, tw, gy, gy + L, c_crt);
+            for (int i = tid; i < H; i += THREADS) raw[i] = crt(A0[pad(i)], A1[pad(i)], LOGH, c_crt);
+        } else {
+            if (square) product_from<true, 0, LOGH, 0, false, false, true>(A0, A1, tw, nullptr, nullptr, c_crt);
+            else product_from<true, 0, LOGH, 1, true, false, true>(A0, A1, tw, gy + H, gy + L + H, c_crt);
+            for (int i = tid; i < H; i += THREADS)  // d as a two's-complement 64-bit value
+                raw[H + i] = crt_signed(A0[pad(i)], A1[pad(i)], LOGH, c_crt, 0ull);
+        }
+        __syncthreads();
     }
-    __syncthreads();
-    if (square) product_from<true, 0, LOGH, 0, false>(A0, A1, tw, nullptr, nullptr, c_crt);
-    else product_from<true, 0, LOGH, 1, true>(A0, A1, tw, gy, gy + L, c_crt);
-    for (int i = tid; i < H; i += THREADS) raw[i] = crt(A0[pad(i)], A1[pad(i)], LOGH, c_crt);
-    for (int i = tid; i < H; i += THREADS) {
-        const uint32_t v = X[pad(i)];
-        X[pad(i)] = twist<LOGL, 0>(v, i, tw);
-        A1[pad(i)] = twist<LOGL, 1>(v, i, tw);
-    }
-    __syncthreads();
-    if (square) product_from<true, 0, LOGH, 0, false>(X, A1, tw, nullptr, nullptr, c_crt);
-    else product_from<true, 0, LOGH, 1, true>(X, A1, tw, gy + H, gy + L + H, c_crt);
-    for (int i = tid; i < H; i += THREADS)  // d as a two's-complement 64-bit value
-        raw[H + i] = crt_signed(untwist<LOGL, 0>(X[pad(i)], i, tw), untwist<LOGL, 1>(A1[pad(i)], i, tw), LOGH,
-                                c_crt, 0ull);
-    __syncthreads();
     carry_pass<true>(L, 0ull, [&](int i) {
         const int k = i < H ? i : i - H;
         const long long c = (long long)raw[k], d = (long long)raw[H + k];

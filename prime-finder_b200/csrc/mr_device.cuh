@@ -124,9 +124,12 @@ __device__ __forceinline__ void load_tw(const uint32_t *__restrict__ W, const ui
 
 // ZHI: the group's upper half (e >= R/2) is known to be zero and is not read;
 // the lower half holds limbs (< 2p), so the first stage is x, x w.
-template <int PR, int RLOG, int SUB, bool ZHI = false>
+// TSH > 0: the elements are first twisted for a negacyclic transform,
+// element i multiplied by psi^i = ww[i << (TSH - 1)] (Shoup companion wwsh).
+template <int PR, int RLOG, int SUB, bool ZHI = false, int TSH = 0>
 __device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, const uint32_t *tw,
-                                            const uint32_t *tws) {
+                                            const uint32_t *tws, const uint32_t *__restrict__ ww = nullptr,
+                                            const uint32_t *__restrict__ wwsh = nullptr) {
     constexpr int R = 1 << RLOG, NL = ZHI ? R / 2 : R;
     constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
     uint32_t v[R];
@@ -138,6 +141,13 @@ __device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, 
     } else {
 #pragma unroll
         for (int e = 0; e < NL; e++) v[e] = A[pad(base + e * SUB)];
+    }
+    if constexpr (TSH > 0) {
+#pragma unroll
+        for (int e = 0; e < NL; e++) {
+            const int k = (base + e * SUB) << (TSH - 1);
+            v[e] = shoup(v[e], __ldg(ww + k), __ldg(wwsh + k), p);
+        }
     }
 #pragma unroll
     for (int s = 0, t0 = 0; s < RLOG; t0 += R >> (s + 1), s++) {
@@ -166,9 +176,12 @@ __device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, 
     }
 }
 
-template <int PR, int RLOG, int H0>
+// TSH > 0: the results are untwisted, element i multiplied by
+// psi^-i = ww[i << (TSH - 1)] (the inverse of a negacyclic transform).
+template <int PR, int RLOG, int H0, int TSH = 0>
 __device__ __forceinline__ void dit_group_t(uint32_t *__restrict__ A, int base, const uint32_t *tw,
-                                            const uint32_t *tws) {
+                                            const uint32_t *tws, const uint32_t *__restrict__ ww = nullptr,
+                                            const uint32_t *__restrict__ wwsh = nullptr) {
     constexpr int R = 1 << RLOG;
     constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
     uint32_t v[R];
@@ -194,6 +207,13 @@ __device__ __forceinline__ void dit_group_t(uint32_t *__restrict__ A, int base, 
             v[e + half] = red2(x - u + p2, p2);
         }
     }
+    if constexpr (TSH > 0) {
+#pragma unroll
+        for (int e = 0; e < R; e++) {
+            const int k = (base + e * H0) << (TSH - 1);
+            v[e] = shoup(v[e], __ldg(ww + k), __ldg(wwsh + k), p);
+        }
+    }
     if constexpr (H0 % 32 == 0) {
         constexpr int PS = H0 + H0 / 32;
         const int pb = pad(base);
@@ -205,9 +225,11 @@ __device__ __forceinline__ void dit_group_t(uint32_t *__restrict__ A, int base, 
     }
 }
 
-template <int PR, int RLOG, int LOGN, int LH0, int STRIDE, bool ZHI = false>
+template <int PR, int RLOG, int LOGN, int LH0, int STRIDE, bool ZHI = false, int TSH = 0>
 __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint32_t *__restrict__ W,
-                                           const uint32_t *__restrict__ Wsh, int g0) {
+                                           const uint32_t *__restrict__ Wsh, int g0,
+                                           const uint32_t *__restrict__ ww = nullptr,
+                                           const uint32_t *__restrict__ wwsh = nullptr) {
     constexpr int R = 1 << RLOG, H0 = 1 << LH0;
     constexpr int GROUPS = (1 << LOGN) >> RLOG;
     constexpr int SUB = (2 * H0) >> RLOG;
@@ -218,7 +240,7 @@ __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint3
 #pragma unroll 1
         for (int gg = g0; gg < GROUPS; gg += STRIDE) {
             const int block = gg / SUB, j0 = gg % SUB;
-            dif_group_t<PR, RLOG, SUB, ZHI>(A, block * 2 * H0 + j0, ta, tsa);
+            dif_group_t<PR, RLOG, SUB, ZHI, TSH>(A, block * 2 * H0 + j0, ta, tsa, ww, wwsh);
         }
     } else {
 #pragma unroll 1
@@ -226,14 +248,16 @@ __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint3
             const int block = gg / SUB, j0 = gg % SUB;
             if constexpr (RLOG == 4) load_wide<0, PR>(LH0, j0, ta, tsa);
             else load_tw<RLOG, false>(W, Wsh, j0, SUB, LH0, ta, tsa);
-            dif_group_t<PR, RLOG, SUB, ZHI>(A, block * 2 * H0 + j0, ta, tsa);
+            dif_group_t<PR, RLOG, SUB, ZHI, TSH>(A, block * 2 * H0 + j0, ta, tsa, ww, wwsh);
         }
     }
 }
 
-template <int PR, int RLOG, int LOGN, int LH0, int STRIDE>
+template <int PR, int RLOG, int LOGN, int LH0, int STRIDE, int TSH = 0>
 __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint32_t *__restrict__ W,
-                                           const uint32_t *__restrict__ Wsh, int g0) {
+                                           const uint32_t *__restrict__ Wsh, int g0,
+                                           const uint32_t *__restrict__ ww = nullptr,
+                                           const uint32_t *__restrict__ wwsh = nullptr) {
     constexpr int R = 1 << RLOG, H0 = 1 << LH0;
     constexpr int GROUPS = (1 << LOGN) >> RLOG;
     uint32_t ta[R - 1], tsa[R - 1];
@@ -243,7 +267,7 @@ __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint3
 #pragma unroll 1
         for (int gg = g0; gg < GROUPS; gg += STRIDE) {
             const int j0 = gg & (H0 - 1);
-            dit_group_t<PR, RLOG, H0>(A, (gg >> LH0) * R * H0 + j0, ta, tsa);
+            dit_group_t<PR, RLOG, H0, TSH>(A, (gg >> LH0) * R * H0 + j0, ta, tsa, ww, wwsh);
         }
     } else {
 #pragma unroll 1
@@ -251,7 +275,7 @@ __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint3
             const int j0 = gg & (H0 - 1);
             if constexpr (RLOG == 4) load_wide<1, PR>(LH0, j0, ta, tsa);
             else load_tw<RLOG, true>(W, Wsh, j0, H0, LH0, ta, tsa);
-            dit_group_t<PR, RLOG, H0>(A, (gg >> LH0) * R * H0 + j0, ta, tsa);
+            dit_group_t<PR, RLOG, H0, TSH>(A, (gg >> LH0) * R * H0 + j0, ta, tsa, ww, wwsh);
         }
     }
 }
@@ -259,20 +283,27 @@ __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint3
 // Forward passes from S remaining stages down (h0 = 2^(S-1)); two primes
 // split the CTA (TWO) or one prime uses all of it.  ZHI (first pass only,
 // S = LOGN): the input's upper half is zero and is neither read nor stored
-// beforehand (a zero-padded operand of a full-length product).
-template <bool TWO, int PR, int LOGN, int S, int STOP = 0, bool ZHI = false>
+// beforehand (a zero-padded operand of a full-length product).  NEG: a
+// negacyclic transform, the first pass twisting its inputs by psi^i (psi a
+// primitive 2^(LOGN+1)-th root of unity).
+template <bool TWO, int PR, int LOGN, int S, int STOP = 0, bool ZHI = false, bool NEG = false>
 __device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
     static_assert(!ZHI || (S == LOGN && S >= 4), "ZHI: first radix-16 pass of the transform");
+    static_assert(!NEG || (S == LOGN && S > STOP && LOGN < LOG_LMAX), "NEG: a forward pass to twist in");
     if constexpr (S > STOP) {
         constexpr int RLOG = S >= 4 ? 4 : S;
+        constexpr int TSH = NEG ? LOG_LMAX - LOGN : 0;  // shift + 1
         if constexpr (TWO) {
             constexpr int half = THREADS / 2;
             if ((int)threadIdx.x < half)
-                dif_pass_t<0, RLOG, LOGN, S - 1, half, ZHI>(A0, tw.w[0], tw.wsh[0], threadIdx.x);
+                dif_pass_t<0, RLOG, LOGN, S - 1, half, ZHI, TSH>(A0, tw.w[0], tw.wsh[0], threadIdx.x, tw.w[0],
+                                                                  tw.wsh[0]);
             else
-                dif_pass_t<1, RLOG, LOGN, S - 1, half, ZHI>(A1, tw.w[1], tw.wsh[1], threadIdx.x - half);
+                dif_pass_t<1, RLOG, LOGN, S - 1, half, ZHI, TSH>(A1, tw.w[1], tw.wsh[1], threadIdx.x - half, tw.w[1],
+                                                                  tw.wsh[1]);
         } else {
-            dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS, ZHI>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x);
+            dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS, ZHI, TSH>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x, tw.w[PR],
+                                                                  tw.wsh[PR]);
         }
         __syncthreads();
         dif_from<TWO, PR, LOGN, S - RLOG, STOP>(A0, A1, tw);
@@ -280,21 +311,25 @@ __device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twidd
 }
 
 // Inverse passes from h0 = 2^LH0 up; the remainder pass (LOGN mod 4) first.
-template <bool TWO, int PR, int LOGN, int LH0>
+// NEG: the last pass untwists its results by psi^-i.
+template <bool TWO, int PR, int LOGN, int LH0, bool NEG = false>
 __device__ __forceinline__ void dit_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
     if constexpr (LH0 < LOGN) {
         constexpr int RLOG = (LH0 == 0 && (LOGN & 3)) ? (LOGN & 3) : 4;
+        constexpr int TSH = (NEG && LH0 + RLOG == LOGN) ? LOG_LMAX - LOGN : 0;
         if constexpr (TWO) {
             constexpr int half = THREADS / 2;
             if ((int)threadIdx.x < half)
-                dit_pass_t<0, RLOG, LOGN, LH0, half>(A0, tw.wi[0], tw.wish[0], threadIdx.x);
+                dit_pass_t<0, RLOG, LOGN, LH0, half, TSH>(A0, tw.wi[0], tw.wish[0], threadIdx.x, tw.wi[0], tw.wish[0]);
             else
-                dit_pass_t<1, RLOG, LOGN, LH0, half>(A1, tw.wi[1], tw.wish[1], threadIdx.x - half);
+                dit_pass_t<1, RLOG, LOGN, LH0, half, TSH>(A1, tw.wi[1], tw.wish[1], threadIdx.x - half, tw.wi[1],
+                                                           tw.wish[1]);
         } else {
-            dit_pass_t<PR, RLOG, LOGN, LH0, THREADS>(A0, tw.wi[PR], tw.wish[PR], threadIdx.x);
+            dit_pass_t<PR, RLOG, LOGN, LH0, THREADS, TSH>(A0, tw.wi[PR], tw.wish[PR], threadIdx.x, tw.wi[PR],
+                                                          tw.wish[PR]);
         }
         __syncthreads();
-        dit_from<TWO, PR, LOGN, LH0 + RLOG>(A0, A1, tw);
+        dit_from<TWO, PR, LOGN, LH0 + RLOG, NEG>(A0, A1, tw);
     }
 }
 
@@ -370,11 +405,13 @@ __device__ __forceinline__ void mid_pass_t(uint32_t *__restrict__ A, const Twidd
 // 2^LOGN: all forward passes but the last, the fused middle sweep, all
 // inverse passes but the first.  C0/C1: the stored spectra of the two primes
 // (OP 1).  ZHI: the operand's upper half is zero and was never stored.
-template <bool TWO, int PR, int LOGN, int OP, bool CG, bool ZHI = false>
+// NEG: negacyclic (twist in the first forward pass, untwist in the last
+// inverse pass; needs at least one pass on each side of the middle sweep).
+template <bool TWO, int PR, int LOGN, int OP, bool CG, bool ZHI = false, bool NEG = false>
 __device__ __forceinline__ void product_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw, const uint32_t *C0,
                                              const uint32_t *C1, const CrtConsts &cc) {
     constexpr int M = mid_rlog<LOGN>();
-    dif_from<TWO, PR, LOGN, LOGN, M, ZHI>(A0, A1, tw);
+    dif_from<TWO, PR, LOGN, LOGN, M, ZHI, NEG>(A0, A1, tw);
     if constexpr (TWO) {
         constexpr int half = THREADS / 2;
         if ((int)threadIdx.x < half) mid_pass_t<0, LOGN, OP, CG, half>(A0, tw, C0, threadIdx.x, cc);
@@ -383,7 +420,7 @@ __device__ __forceinline__ void product_from(uint32_t *A0, uint32_t *A1, const T
         mid_pass_t<PR, LOGN, OP, CG, THREADS>(A0, tw, C0, threadIdx.x, cc);
     }
     __syncthreads();
-    dit_from<TWO, PR, LOGN, M>(A0, A1, tw);
+    dit_from<TWO, PR, LOGN, M, NEG>(A0, A1, tw);
 }
 
 #define PFB_LOGN_CASES(F) \
@@ -580,28 +617,13 @@ struct Cand {
     int logl;
 };
 
-// Shared-memory view of one step: three transform buffers of H padded words
-// (A0, A1, X; X holds the residue between steps) and the carry scratch.
+// Shared-memory view of one step: transform buffers A0, A1 (L padded words
+// each up to L = 2^LOG_LCTA, H above), the residue X (H padded words) and
+// the carry scratch.
 struct Smem {
     uint32_t *A0, *A1, *X;
     CarrySmem *cs;
 };
-
-// Negacyclic transforms of length H are cyclic ones of the input twisted by
-// psi^i, psi = omega_L a primitive 2H-th root of unity (the upper half of
-// the length-L transform of a zero-padded input); the inverse untwists by
-// psi^-i.  psi^i = w[i 2^(LOG_LMAX - LOGL)], within the table's half circle.
-template <int LOGL, int PR>
-__device__ __forceinline__ uint32_t twist(uint32_t v, int i, const Twiddles &tw) {
-    const int k = i << (LOG_LMAX - LOGL);
-    return shoup(v, __ldg(tw.w[PR] + k), __ldg(tw.wsh[PR] + k), PR ? P2 : P1);
-}
-
-template <int LOGL, int PR>
-__device__ __forceinline__ uint32_t untwist(uint32_t v, int i, const Twiddles &tw) {
-    const int k = i << (LOG_LMAX - LOGL);
-    return shoup(v, __ldg(tw.wi[PR] + k), __ldg(tw.wish[PR] + k), PR ? P2 : P1);
-}
 
 // Signed coefficients.  A product of two H-coefficient operands with limbs in
 // (-2^22, 2^22 + 2) has coefficients c with |c| < H 2^44 (1 + 2^-20) < P12/2
@@ -623,97 +645,126 @@ __device__ __forceinline__ unsigned long long crt_signed(uint32_t r1, uint32_t r
 // One Montgomery step on X (H limbs of 22 bits), with the Montgomery radix
 // R' = B^H + 1 (B = 2^22):
 //   X <- REDC(X^2) * a      (square = true)
-//   X <- REDC(X * Y) * a    (gy = spectrum of Y: cyclic half and negacyclic half, see spectrum)
+//   X <- REDC(X * Y) * a    (gy = spectrum of Y, the length-L transform of its
+//                            zero-padded limbs: cyclic half, negacyclic half)
 //   X <- REDC(X) * a        (square = false, no gy)
-// REDC(T) = (T + m N) / R' with m = -T N^-1 mod R' in [0, R').  Every
-// product is of length H, both primes in shared memory at once:
-//   S = T mod (B^H - 1)     cyclic square (or product)
-//   D = T mod (B^H + 1)     negacyclic square (or product)
-//   m = D N'' mod (B^H + 1) negacyclic product with the stored spectrum of N''
-//   W = m N mod (B^H - 1)   cyclic product with the stored spectrum of N
+// REDC(T) = (T + m N) / R' with m = -T N^-1 mod R' in [0, R'):
+//   S = T mod (B^H - 1),  D = T mod (B^H + 1)
+//   m = D N'' mod (B^H + 1)   negacyclic product with the stored spectrum of N''
+//   W = m N mod (B^H - 1)     cyclic product with the stored spectrum of N
 //   V = S + W mod (B^H - 1)
-// Since R' == 2 (mod B^H - 1), V == 2 U for U = REDC(T); U < 2N and 4N <
-// B^H - 1 make V = 2U exactly, so a U is (a/2) V for even a (the base-2
-// ladder's multiply by 2 costs nothing) and a (V >> 1) for odd a.  That is 4
-// length-L-equivalent transforms per step where a radix R = B^H needs 5 (its
-// m = (T mod R) N' mod R is a zero-padded length-L product).
+// Up to L = 2^LOG_LCTA, T comes from one zero-padded length-L product, S and
+// D from its halves (S = T_lo + T_hi, D = T_lo - T_hi, no carry needed for D);
+// at L = 2^15 both primes of a length-L transform do not fit one CTA, so S and
+// D come from a cyclic and a negacyclic product of length H (the two halves of
+// that transform, computed apart).  Since R' == 2 (mod B^H - 1), V == 2U for
+// U = REDC(T); U < 2N and 4N < B^H - 1 make V = 2U exactly, so a U is (a/2) V
+// for even a (the base-2 ladder's multiply by 2 costs nothing) and a (V >> 1)
+// for odd a.  That is 4 length-L-equivalent transforms per step where the
+// radix B^H needs 5 (its m = (T mod B^H) N' mod B^H is a zero-padded
+// length-L product).
 // On entry X, Y < c N with R' > 4 c^2 N (c = 4 for the strong test), or
-// X < R' for a plain REDC; on exit X < 2N * a.  A1 and A0 are clobbered.
+// X < R' for a plain REDC; on exit X < 2N * a.  A0 and A1 are clobbered.
 template <bool MUL, int LOGL>
 __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
                           const CrtConsts &cc, const uint32_t *gy = nullptr) {
     constexpr int L = 1 << LOGL, H = L >> 1, LOGH = LOGL - 1;
     constexpr int T = THREADS;
+    constexpr bool FULL = LOGL <= LOG_LCTA;  // T from one length-L product
     uint32_t *A0 = sm.A0, *A1 = sm.A1, *X = sm.X;
+    // the m and W products run on (P, Q); S waits in Sb until the end
+    uint32_t *const P = FULL ? A0 : X, *const Q = A1, *const Sb = FULL ? X : A0;
     CarrySmem &cs = *sm.cs;
     const int tid = threadIdx.x;
-    unsigned long long cS = 0, cD = 0;
-    if (square || (MUL && gy)) {
-        // S: cyclic product, A0 (prime 1) and A1 (prime 2); carried into A0
-        for (int i = tid; i < H; i += T) {
-            const uint32_t v = X[pad(i)];
-            A0[pad(i)] = v;
-            A1[pad(i)] = v;
+    const bool prod = square || (MUL && gy);
+    unsigned long long cS = 0;
+    if constexpr (FULL) {
+        if (prod) {
+            for (int i = tid; i < H; i += T) {
+                const uint32_t v = X[pad(i)];
+                A0[pad(i)] = v;
+                A1[pad(i)] = v;
+            }
+            __syncthreads();
+            if (MUL && gy) product_from<true, 0, LOGL, 1, true, true>(A0, A1, tw, gy, gy + L, cc);
+            else product_from<true, 0, LOGL, 0, false, true>(A0, A1, tw, nullptr, nullptr, cc);
+            carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], LOGL, cc); }, A0, cs);
+            cS = carry_pass<true>(H, 0ull,
+                                  [&](int i) { return (unsigned long long)A0[pad(i)] + A0[pad(i + H)]; }, X, cs);
+            for (int i = tid; i < H; i += T) {  // D = T_lo - T_hi, limbs in (-B, B)
+                const uint32_t lo = A0[pad(i)], hi = A0[pad(i + H)];
+                A0[pad(i)] = lo + P1 - hi;
+                A1[pad(i)] = lo + P2 - hi;
+            }
+        } else {  // T = X: S = D = X
+            for (int i = tid; i < H; i += T) {
+                const uint32_t v = X[pad(i)];
+                A0[pad(i)] = v;
+                A1[pad(i)] = v;
+            }
         }
         __syncthreads();
-        if (MUL && gy) product_from<true, 0, LOGH, 1, true>(A0, A1, tw, gy, gy + L, cc);
-        else product_from<true, 0, LOGH, 0, false>(A0, A1, tw, nullptr, nullptr, cc);
-        cS = carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], LOGH, cc); }, A0, cs);
-        // D: negacyclic product, X itself (prime 1) and A1 (prime 2); carried into X
-        for (int i = tid; i < H; i += T) {
-            const uint32_t v = X[pad(i)];
-            X[pad(i)] = twist<LOGL, 0>(v, i, tw);
-            A1[pad(i)] = twist<LOGL, 1>(v, i, tw);
-        }
-        __syncthreads();
-        if (MUL && gy) product_from<true, 0, LOGH, 1, true>(X, A1, tw, gy + H, gy + L + H, cc);
-        else product_from<true, 0, LOGH, 0, false>(X, A1, tw, nullptr, nullptr, cc);
-        cD = carry_pass<true>(H, 0ull, [&](int i) {
-            return crt_signed(untwist<LOGL, 0>(X[pad(i)], i, tw), untwist<LOGL, 1>(A1[pad(i)], i, tw), LOGH, cc,
-                              i == 0 ? OFF_N0 : OFF_C);
-        }, X, cs);
     } else {
-        // T = X: S = D = X
-        for (int i = tid; i < H; i += T) A0[pad(i)] = X[pad(i)];
-        __syncthreads();
-    }
-    // m: D == X - cD (mod B^H + 1), cD < 2^39 folded into limbs 0 and 1
-    // (signed limbs, represented mod p)
-    unsigned long long cM;
-    {
-        const uint32_t c0 = (uint32_t)cD & LIMB_MASK, c1 = (uint32_t)(cD >> LIMB_BITS);
-        for (int i = tid; i < H; i += T) {
-            const uint32_t v = X[pad(i)], c = i == 0 ? c0 : (i == 1 ? c1 : 0u);
-            X[pad(i)] = twist<LOGL, 0>(v + P1 - c, i, tw);
-            A1[pad(i)] = twist<LOGL, 1>(v + P2 - c, i, tw);
+        if (prod) {
+            // S: cyclic product in A0 (prime 1) and A1 (prime 2), kept in A0
+            for (int i = tid; i < H; i += T) {
+                const uint32_t v = X[pad(i)];
+                A0[pad(i)] = v;
+                A1[pad(i)] = v;
+            }
+            __syncthreads();
+            if (MUL && gy) product_from<true, 0, LOGH, 1, true>(A0, A1, tw, gy, gy + L, cc);
+            else product_from<true, 0, LOGH, 0, false>(A0, A1, tw, nullptr, nullptr, cc);
+            cS = carry_pass<true>(H, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], LOGH, cc); }, A0, cs);
+            // D: negacyclic product in X itself (prime 1) and A1 (prime 2), carried into X
+            for (int i = tid; i < H; i += T) A1[pad(i)] = X[pad(i)];
+            __syncthreads();
+            if (MUL && gy) product_from<true, 0, LOGH, 1, true, false, true>(X, A1, tw, gy + H, gy + L + H, cc);
+            else product_from<true, 0, LOGH, 0, false, false, true>(X, A1, tw, nullptr, nullptr, cc);
+            const unsigned long long cD = carry_pass<true>(H, 0ull, [&](int i) {
+                return crt_signed(X[pad(i)], A1[pad(i)], LOGH, cc, i == 0 ? OFF_N0 : OFF_C);
+            }, X, cs);
+            // D == X - cD (mod B^H + 1): cD < 2^39 folded into limbs 0 and 1 (signed limbs, mod p)
+            const uint32_t c0 = (uint32_t)cD & LIMB_MASK, c1 = (uint32_t)(cD >> LIMB_BITS);
+            for (int i = tid; i < H; i += T) {
+                const uint32_t v = X[pad(i)], c = i == 0 ? c0 : (i == 1 ? c1 : 0u);
+                X[pad(i)] = v + P1 - c;
+                A1[pad(i)] = v + P2 - c;
+            }
+        } else {  // T = X: S = D = X
+            for (int i = tid; i < H; i += T) {
+                const uint32_t v = X[pad(i)];
+                A0[pad(i)] = v;
+                A1[pad(i)] = v;
+            }
         }
         __syncthreads();
-        product_from<true, 0, LOGH, 1, false>(X, A1, tw, cd.nn, cd.nn + H, cc);
-        cM = carry_pass<true>(H, 0ull, [&](int i) {
-            return crt_signed(untwist<LOGL, 0>(X[pad(i)], i, tw), untwist<LOGL, 1>(A1[pad(i)], i, tw), LOGH, cc,
-                              i == 0 ? OFF_N0 : OFF_C);
-        }, X, cs);
     }
-    // m = lo - cM, plus R' when lo < cM (lo: the H limbs in X); modulo
+    // m = D N'' (mod B^H + 1): negacyclic product on (P, Q), carried into P
+    product_from<true, 0, LOGH, 1, false, false, true>(P, Q, tw, cd.nn, cd.nn + H, cc);
+    const unsigned long long cM = carry_pass<true>(H, 0ull, [&](int i) {
+        return crt_signed(P[pad(i)], Q[pad(i)], LOGH, cc, i == 0 ? OFF_N0 : OFF_C);
+    }, P, cs);
+    // m = lo - cM, plus R' when lo < cM (lo: the H limbs in P); modulo
     // B^H - 1 that is lo - cM + 2 neg
     bool z = true;
-    for (int i = tid; i < H; i += T) z = z && (i < 2 || X[pad(i)] == 0u);
+    for (int i = tid; i < H; i += T) z = z && (i < 2 || P[pad(i)] == 0u);
     const bool upper_zero = __syncthreads_and(z) != 0;
-    const bool neg = upper_zero && ((((unsigned long long)X[pad(1)] << LIMB_BITS) | X[pad(0)]) < cM);
+    const bool neg = upper_zero && ((((unsigned long long)P[pad(1)] << LIMB_BITS) | P[pad(0)]) < cM);
     __syncthreads();
     {
         const uint32_t m0 = (uint32_t)cM & LIMB_MASK, m1 = (uint32_t)(cM >> LIMB_BITS);
         for (int i = tid; i < H; i += T) {
-            const uint32_t v = X[pad(i)] + (i == 0 && neg ? 2u : 0u), c = i == 0 ? m0 : (i == 1 ? m1 : 0u);
-            X[pad(i)] = v + P1 - c;
-            A1[pad(i)] = v + P2 - c;
+            const uint32_t v = P[pad(i)] + (i == 0 && neg ? 2u : 0u), c = i == 0 ? m0 : (i == 1 ? m1 : 0u);
+            P[pad(i)] = v + P1 - c;
+            Q[pad(i)] = v + P2 - c;
         }
         __syncthreads();
     }
-    // W = m N (mod B^H - 1), then V = S + W into X; end-around carries
-    product_from<true, 0, LOGH, 1, false>(X, A1, tw, cd.nh, cd.nh + H, cc);
+    // W = m N (mod B^H - 1) on (P, Q), then V = S + W into X; end-around carries
+    product_from<true, 0, LOGH, 1, false>(P, Q, tw, cd.nh, cd.nh + H, cc);
     unsigned long long c = carry_pass<true>(H, cS, [&](int i) {
-        return (unsigned long long)A0[pad(i)] + crt_signed(X[pad(i)], A1[pad(i)], LOGH, cc, OFF_C);
+        return (unsigned long long)Sb[pad(i)] + crt_signed(P[pad(i)], Q[pad(i)], LOGH, cc, OFF_C);
     }, X, cs);
     while (c) c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
     // V = B^H - 1 represents 0 (U = 0: T = 0)

@@ -44,23 +44,25 @@ struct LucasDev {
     uint32_t lb;  // every stored value is < lb * N
 };
 
-// Shared memory: three transform buffers of H padded words (A0, A1, X) and,
-// up to L = 2^LOG_LCTA, a fourth for the residue Y (at L = 2^15, Y lives in
-// the candidate's global ybuf).
+// Shared memory: up to L = 2^LOG_LCTA both primes' length-L transforms (A0,
+// A1), the residue X and a second residue Y; at L = 2^15 three buffers of H
+// padded words (A0, A1, X; every product there is of length H) and Y in the
+// candidate's global ybuf.
 __host__ __device__ inline size_t smem_words(int logl) {
-    const size_t H = (size_t)1 << (logl - 1), B = H + H / 32;
-    return (logl <= LOG_LCTA ? 4 : 3) * B;
+    const size_t L = (size_t)1 << logl, H = L / 2;
+    return logl <= LOG_LCTA ? 2 * (L + L / 32) + 2 * (H + H / 32) : 3 * (H + H / 32);
 }
 inline size_t smem_bytes(int logl) {
     return smem_words(logl) * sizeof(uint32_t) + sizeof(CarrySmem) + 16;
 }
 
 __device__ __forceinline__ void carve(uint32_t *raw, int logl, Smem &sm, uint32_t *&Y, uint32_t *ybuf) {
-    const int H = 1 << (logl - 1), B = H + H / 32;
+    const int L = 1 << logl, H = L >> 1;
+    const int BA = logl <= LOG_LCTA ? L + L / 32 : H + H / 32, BX = H + H / 32;
     sm.A0 = raw;
-    sm.A1 = raw + B;
-    sm.X = raw + 2 * B;
-    Y = logl <= LOG_LCTA ? raw + 3 * B : ybuf;
+    sm.A1 = raw + BA;
+    sm.X = raw + 2 * BA;
+    Y = logl <= LOG_LCTA ? sm.X + BX : ybuf;
     uintptr_t c = (uintptr_t)(raw + smem_words(logl));
     c = (c + 15) & ~(uintptr_t)15;
     sm.cs = (CarrySmem *)c;
@@ -79,11 +81,12 @@ __device__ void spectra_t(const Smem &sm, const uint32_t *src, uint32_t *gc1, ui
         if (!g1) continue;
         for (int i = tid; i < H; i += THREADS) {
             const uint32_t v = cg ? __ldcg(src + i) : src[i];
-            sm.A0[pad(i)] = neg ? twist<LOGL, 0>(v, i, tw) : v;
-            sm.A1[pad(i)] = neg ? twist<LOGL, 1>(v, i, tw) : v;
+            sm.A0[pad(i)] = v;
+            sm.A1[pad(i)] = v;
         }
         __syncthreads();
-        dif_from<true, 0, LOGH, LOGH>(sm.A0, sm.A1, tw);
+        if (neg) dif_from<true, 0, LOGH, LOGH, 0, false, true>(sm.A0, sm.A1, tw);
+        else dif_from<true, 0, LOGH, LOGH>(sm.A0, sm.A1, tw);
         for (int i = tid; i < H; i += THREADS) {
             g1[i] = red2(sm.A0[pad(i)], P1);
             g2[i] = red2(sm.A1[pad(i)], P2);

@@ -485,6 +485,8 @@ def _server_lib():
         L.pfb_mr_server_stats.restype = C.c_int
         L.pfb_mr_server_destroy.argtypes = [vp]
         L.pfb_mr_server_destroy.restype = None
+        L.pfb_mr_server_inject_alloc_failures.argtypes = [vp, C.c_int]
+        L.pfb_mr_server_inject_alloc_failures.restype = C.c_int
         L.pfb_mr_batch_steps_done.argtypes = [vp]
         L.pfb_mr_batch_steps_done.restype = C.c_longlong
         L._server_ready = True
@@ -529,6 +531,14 @@ class MRServer:
                 d["residue"] = limbs16_to_int(rb)
             res.append(d)
         return res
+
+    def inject_alloc_failures(self, n: int) -> int:
+        """Test hook: the next n slot allocations fail on the host as if the
+        device were out of memory; returns the injected failures consumed."""
+        rc = _server_lib().pfb_mr_server_inject_alloc_failures(self._h, n)
+        if rc < 0:
+            raise PfbError(rc, "pfb_mr_server_inject_alloc_failures")
+        return rc
 
     def stats(self) -> dict:
         st = ServerStats()

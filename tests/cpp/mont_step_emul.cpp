@@ -119,8 +119,8 @@ int main() {
         pfb::big::to_limbs(N, LIMB_BITS, nl.data(), H);
         pfb::big::to_limbs(x, LIMB_BITS, xl.data(), H);
         pfb::big::to_limbs(Y, LIMB_BITS, yl.data(), H);
-        const int B = H + H / 32;
-        std::vector<uint32_t> A0(B), A1(B), X(B);
+        const int B = H + H / 32, BA = logl <= LOG_LCTA ? L + L / 32 : B;
+        std::vector<uint32_t> A0(BA), A1(BA), X(B);
         std::vector<uint32_t> nn(2 * H), nh(2 * H), gy(2 * L);
         CarrySmem cs{};
         const Smem sm{A0.data(), A1.data(), X.data(), &cs};

@@ -120,3 +120,38 @@ def test_full_size_requests_in_the_mix(engine):
         assert "%016x" % (x & (2**64 - 1)) == r["low64"], i
         assert hashlib.sha256(x.to_bytes(2 * n16, "little")).hexdigest() == r["sha256"], i
         assert got[i]["verdict"] == r["sprp2"]
+
+
+def test_slot_allocation_failure_recovery(engine):
+    """The server's recovery when slot memory cannot be allocated, driven by
+    host-side fault injection (pfb_mr_server_inject_alloc_failures; the
+    device never faults): with nothing resident, a request whose allocation
+    and retry both fail is reported with verdict -1; with candidates
+    resident, it is requeued and admitted once memory comes back, and its
+    residue still equals GMP's."""
+    rng = random.Random(17)
+    srv = pfb200.MRServer(engine, max_resident=8, chunk_steps=256)
+    assert srv.inject_alloc_failures(2) == 0
+    srv.submit(rng.getrandbits(3000) | 1 | (1 << 2999), tag=0, residue=True)
+    got = _drain(srv, 1, 60)
+    assert got[0]["verdict"] == -1
+    assert srv.inject_alloc_failures(0) == 2
+    # two long requests become resident; then three allocations fail
+    longs = [rng.getrandbits(60000) | 1 | (1 << 59999) for _ in range(2)]
+    for i, N in enumerate(longs):
+        srv.submit(N, tag=10 + i, residue=True)
+    t0 = time.time()
+    while srv.stats()["resident"] < 2 and time.time() - t0 < 60:
+        time.sleep(0.01)
+    assert srv.stats()["resident"] == 2
+    srv.inject_alloc_failures(3)
+    shorts = [rng.getrandbits(b) | 1 | (1 << (b - 1)) for b in (2000, 5000, 9000)]
+    for i, N in enumerate(shorts):
+        srv.submit(N, tag=20 + i, residue=True)
+    got = _drain(srv, 5, 300)
+    used = srv.inject_alloc_failures(0)
+    srv.close()
+    assert used == 5 and len(got) == 5
+    for tag, N in list(zip((10, 11), longs)) + list(zip((20, 21, 22), shorts)):
+        assert got[tag]["verdict"] == oracle.strong_test(N, 2)
+        assert got[tag]["residue"] == oracle.strong_residue(N, 2)[1]

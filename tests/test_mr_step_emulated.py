@@ -12,11 +12,12 @@ U = (T + m N) / R', the step leaves U * a for T = x^2 (squaring), T = x y
 (general product through y's stored spectrum, the Lucas test's form) or
 T = x (conversion out of Montgomery form).
 
-This pins the arithmetic of the cyclic and negacyclic transforms (the twist
-by a 2H-th root of unity), the fused pointwise sweep, the signed CRT with its
-offsets, the carry-lookahead passes, the end-around carry and the halving
-of V = 2U at the transform lengths 2^8, 2^9, 2^10, 2^14 and 2^15 (every
-length keeps both primes in one CTA).
+This pins the arithmetic of the transforms (the zero-padded length-L product
+up to 2^14; at 2^15 the cyclic and negacyclic halves of length H, the twist
+by a 2H-th root of unity fused into the first and last passes), the fused
+pointwise sweep, the signed CRT with its offsets, the carry-lookahead passes,
+the end-around carry and the halving of V = 2U at the transform lengths 2^8,
+2^9, 2^10, 2^14 and 2^15.
 It does not stand in for the GPU tests: timing, memory ordering between
 CTAs and the scheduler are not emulated.
 """
