@@ -299,6 +299,22 @@ def sieve_case():
     sv.close()
 
 
+def radix_case(ctas=592, reps=20):
+    """The first radix-16 pass of a 2^14-point transform (both primes, 592
+    CTAs = 4 per SM of work, each on its own random limbs) as the engine's
+    butterfly pass and as an exact int8 byte-plane product on the tensor
+    cores; the two forms' outputs must agree word for word."""
+    import pfb200
+    eng = pfb200.MillerRabin(0)
+    r = pfb200.radix16_forms(eng, ctas, reps)
+    eng.close()
+    n = 1 << 14
+    r.update({"case": "radix-16 pass, 2^14 points, 2 primes", "ctas": ctas,
+              "points_per_s_butterfly": ctas * 2 * n / (r["ms_butterfly"] / 1e3),
+              "points_per_s_tensor": ctas * 2 * n / (r["ms_tensor"] / 1e3) if r["ms_tensor"] > 0 else None})
+    print(json.dumps(r))
+
+
 # small cases of the squaring kernel for ncu captures: N and rev(N) of four
 # (k, j) at one (a, b, c), 8 candidates (one CTA each), one launch of 64 squarings
 MR_CASES = {
@@ -362,7 +378,12 @@ def main():
                     help="also time the stages of the e2e call apart (one more e2e-sized run)")
     ap.add_argument("--sieve-case", action="store_true",
                     help="only run one K = 9999 sieve triple twice (for ncu)")
+    ap.add_argument("--radix-case", action="store_true",
+                    help="only time one radix-16 transform pass in its butterfly and tensor-core forms")
     args = ap.parse_args()
+    if args.radix_case:
+        radix_case()
+        return
     if args.sieve_case:
         sieve_case()
         return

@@ -217,6 +217,19 @@ long long pfb_mr_test_cost(const uint16_t *limbs, int n_limbs);
 int pfb_measure_int32_peak(int device, double *mul_lo_per_s, double *mul_hi_per_s);
 
 /*
+ * Measurement utility (no counterpart in the reference): one radix-16 pass of
+ * the squaring kernel's transform -- the first forward pass of a 2^14-point
+ * transform, both primes -- in two forms on `ctas` CTAs, each on its own
+ * 2^14 random limbs: the engine's butterfly pass (integer pipe) and an exact
+ * int8 byte-plane matrix product on the tensor cores (tcgen05.mma kind::i8)
+ * with the recombination on the CUDA cores.  Writes the mean time of one
+ * launch of each form over `reps` launches, the number of output words on
+ * which the two forms differ, and the tensor form's wait-timeout flag.
+ */
+int pfb_mr_radix16_forms(pfb_mr_t *e, int ctas, int reps, double *ms_butterfly, double *ms_tensor,
+                         long long *mismatches, int *tensor_error);
+
+/*
  * Autotuner of the persistent squaring kernel, per transform-length bucket
  * (log2 L from logl_lo to logl_hi, within 8..15; a 50 000-digit modulus is
  * 14, 100 000 digits 15).  For each bucket it times 2048 squarings of

@@ -21,6 +21,7 @@
 
 #include "mr_ctx_kernels.cuh"
 #include "mr_kernels.cuh"
+#include "radix_probe.cuh"
 #include "mr_prep_host.h"
 
 using namespace pfb::mr;
@@ -1404,4 +1405,123 @@ extern "C" int pfb_mr_ctx_sq_raw(pfb_mr_ctx_t *c, const uint64_t *d_a, uint64_t 
 extern "C" int pfb_mr_ctx_mul_raw(pfb_mr_ctx_t *c, const uint64_t *d_a, const uint64_t *d_b, uint64_t *d_out,
                                   void *stream) {
     return ctx_launch(c, d_a, d_b, d_out, c ? 2 * c->n16 + 16 : 0, CTX_RAW_MUL, stream);
+}
+
+// ---------------------------------------------------------------------------
+// Measurement: two forms of one radix-16 pass (radix_probe.cuh).
+
+extern "C" int pfb_mr_radix16_forms(pfb_mr_t *e, int ctas, int reps, double *ms_butterfly, double *ms_tensor,
+                                    long long *mismatches, int *tensor_error) {
+    if (!e || ctas <= 0 || reps <= 0 || !ms_butterfly || !ms_tensor || !mismatches || !tensor_error) {
+        pfb::set_error("pfb_mr_radix16_forms: bad argument");
+        return PFB_E_ARG;
+    }
+    PFB_CUDA(cudaSetDevice(e->device));
+    const uint32_t P[2] = {P1, P2};
+    // host tables: the operand image of the byte planes of F, omega_n^t, floor(2^64 / p)
+    std::vector<uint8_t> fa(RP_OPND, 0);
+    std::vector<uint32_t> wn(4 * (size_t)RP_N);
+    RpTables t{};
+    for (int pr = 0; pr < 2; pr++) {
+        const uint64_t p = P[pr];
+        uint64_t om = 1, b = 3, ex = (p - 1) >> LOG_LMAX;  // order 2^15
+        for (; ex; ex >>= 1, b = b * b % p)
+            if (ex & 1) om = om * b % p;
+        const uint64_t wn1 = om * om % p;  // order 2^14
+        uint64_t w16 = 1;
+        for (int i = 0; i < RP_N / 16; i++) w16 = w16 * wn1 % p;  // order 16
+        uint32_t *wv = wn.data() + (size_t)(2 * pr) * RP_N, *ws = wv + RP_N;
+        uint64_t a = 1;
+        for (int i = 0; i < RP_N; i++, a = a * wn1 % p) {
+            wv[i] = (uint32_t)a;
+            ws[i] = (uint32_t)(((uint64_t)a << 32) / p);
+        }
+        for (int k = 0; k < 16; k++) {
+            uint64_t wk = 1;
+            for (int i = 0; i < k; i++) wk = wk * w16 % p;
+            uint64_t f = 1;
+            for (int m = 0; m < 16; m++, f = f * wk % p)
+                for (int byte = 0; byte < 4; byte++) fa[rp_off(pr * 64 + k * 4 + byte, m)] = (uint8_t)(f >> (8 * byte));
+        }
+        t.mu[pr] = ~0ull / p;
+    }
+    const size_t nx = (size_t)ctas * RP_N;
+    uint32_t *d_x = nullptr, *d_yb = nullptr, *d_yt = nullptr, *d_wn = nullptr;
+    uint8_t *d_fa = nullptr;
+    int *d_err = nullptr;
+    cudaError_t ce = cudaMalloc(&d_x, nx * 4);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_yb, 2 * nx * 4);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_yt, 2 * nx * 4);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_wn, wn.size() * 4);
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_fa, fa.size());
+    if (ce == cudaSuccess) ce = cudaMalloc(&d_err, sizeof(int));
+    auto release = [&]() {
+        cudaFree(d_x);
+        cudaFree(d_yb);
+        cudaFree(d_yt);
+        cudaFree(d_wn);
+        cudaFree(d_fa);
+        cudaFree(d_err);
+    };
+    if (ce != cudaSuccess) {
+        release();
+        return pfb::cuda_fail(ce, "pfb_mr_radix16_forms: allocation", __FILE__, __LINE__);
+    }
+    std::vector<uint32_t> hx(nx);
+    uint64_t st = 0x9E3779B97F4A7C15ull;
+    for (auto &v : hx) {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        v = (uint32_t)(st >> 40) & LIMB_MASK;
+    }
+    float ms_b = 0.f, ms_t = 0.f;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    do {
+        if ((ce = cudaMemcpy(d_x, hx.data(), nx * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((ce = cudaMemcpy(d_wn, wn.data(), wn.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((ce = cudaMemcpy(d_fa, fa.data(), fa.size(), cudaMemcpyHostToDevice)) != cudaSuccess) break;
+        if ((ce = cudaMemset(d_err, 0, sizeof(int))) != cudaSuccess) break;
+        t.fa = d_fa;
+        for (int pr = 0; pr < 2; pr++) {
+            t.wn[pr] = d_wn + (size_t)(2 * pr) * RP_N;
+            t.wnsh[pr] = t.wn[pr] + RP_N;
+        }
+        const int smem_b = (int)(2 * (RP_N + RP_N / 32) * sizeof(uint32_t));
+        if ((ce = cudaFuncSetAttribute(rp_butterfly_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_b)) !=
+            cudaSuccess)
+            break;
+        if ((ce = cudaFuncSetAttribute(rp_tensor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, RP_SMEM)) !=
+            cudaSuccess)
+            break;
+        if ((ce = cudaEventCreate(&e0)) != cudaSuccess || (ce = cudaEventCreate(&e1)) != cudaSuccess) break;
+        cudaStream_t s = e->stream;
+        for (int form = 0; form < 2 && ce == cudaSuccess; form++) {
+            for (int r = -1; r < reps; r++) {  // one untimed launch first
+                if (r == 0) cudaEventRecord(e0, s);
+                if (form == 0) rp_butterfly_kernel<<<ctas, THREADS, smem_b, s>>>(d_x, d_yb, e->tw);
+                else rp_tensor_kernel<<<ctas, THREADS, RP_SMEM, s>>>(d_x, d_yt, t, d_err);
+            }
+            cudaEventRecord(e1, s);
+            if ((ce = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            if ((ce = cudaGetLastError()) != cudaSuccess) break;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            (form == 0 ? ms_b : ms_t) = ms / reps;
+        }
+        if (ce != cudaSuccess) break;
+        std::vector<uint32_t> yb(2 * nx), yt(2 * nx);
+        if ((ce = cudaMemcpy(yb.data(), d_yb, yb.size() * 4, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+        if ((ce = cudaMemcpy(yt.data(), d_yt, yt.size() * 4, cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+        if ((ce = cudaMemcpy(tensor_error, d_err, sizeof(int), cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+        long long bad = 0;
+        for (size_t i = 0; i < yb.size(); i++) bad += yb[i] != yt[i];
+        *mismatches = bad;
+    } while (0);
+    int rc = PFB_OK;
+    if (ce != cudaSuccess) rc = pfb::cuda_fail(ce, "pfb_mr_radix16_forms", __FILE__, __LINE__);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    release();
+    *ms_butterfly = ms_b;
+    *ms_tensor = ms_t;
+    return rc;
 }

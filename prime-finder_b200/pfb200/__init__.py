@@ -421,6 +421,20 @@ class MRBatch:
             pass
 
 
+def radix16_forms(engine: "MillerRabin", ctas: int = 592, reps: int = 20) -> dict:
+    """One radix-16 transform pass in its butterfly form and as a tensor-core
+    byte-plane product (pfb_mr_radix16_forms): per-launch times, output
+    mismatches between the two forms, the tensor form's timeout flag."""
+    L = _mr_lib()
+    f = L.pfb_mr_radix16_forms
+    f.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
+                  C.POINTER(C.c_longlong), C.POINTER(C.c_int)]
+    f.restype = C.c_int
+    tb, tt, bad, err = C.c_double(), C.c_double(), C.c_longlong(), C.c_int()
+    _check(f(engine._h, ctas, reps, C.byref(tb), C.byref(tt), C.byref(bad), C.byref(err)), "pfb_mr_radix16_forms")
+    return {"ms_butterfly": tb.value, "ms_tensor": tt.value, "mismatches": bad.value, "tensor_timeout": err.value}
+
+
 def measure_int32_peak(device: int = 0):
     """(mul.lo ops/s, mul.hi ops/s) sustained on `device`."""
     lo, hi = C.c_double(0), C.c_double(0)
