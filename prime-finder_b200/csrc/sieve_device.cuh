@@ -179,14 +179,15 @@ __device__ __forceinline__ unsigned long long quot64(unsigned long long n, uint3
     return q;
 }
 
-// The descent keeps, per level, the multiplier a and the interval start L,
-// packed in one 64-bit word (one local-memory store and load per level; the
-// reciprocal of a is recomputed on the way back); the level's modulus is the
-// previous level's multiplier (p at level 0).
+// The descent keeps, per level, the multiplier a and the interval start L
+// packed in one 64-bit word, and the reciprocal of a (one 64-bit store and
+// load each per level); the level's modulus is the previous level's
+// multiplier (p at level 0), which the way back already holds.
 __device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, uint32_t Y) {
     if (c < Y) return 0u;
     uint32_t a = g, m = p, L = p - c, R = p - c + Y - 1u;
     unsigned long long st[34];
+    double sr[34];
     int d = 0;
     uint32_t x;
     for (;;) {
@@ -197,7 +198,9 @@ __device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, u
             break;
         }
         if (d >= 34) return 0xFFFFFFFFu;  // unreachable: the modulus halves each level
-        st[d++] = ((unsigned long long)L << 32) | a;
+        st[d] = ((unsigned long long)L << 32) | a;
+        sr[d] = rd;
+        d++;
         const uint32_t r = m - quot32(m, a, rd) * a;  // != 0: gcd(a, m) = 1 along the chain
         uint32_t a2 = a - r, L2 = L - quot32(L, a, rd) * a, R2 = R - quot32(R, a, rd) * a;
         const uint32_t m2 = a;
@@ -218,7 +221,7 @@ __device__ __noinline__ uint32_t first_hit(uint32_t c, uint32_t g, uint32_t p, u
         const uint32_t ad = (uint32_t)cur, ld = (uint32_t)(cur >> 32);
         const unsigned long long prev = d ? st[d - 1] : (unsigned long long)p;
         const uint32_t md = (uint32_t)prev;
-        x = (uint32_t)quot64((unsigned long long)x * md + ld + ad - 1u, ad, 1.0 / (double)ad);  // ceil
+        x = (uint32_t)quot64((unsigned long long)x * md + ld + ad - 1u, ad, sr[d]);  // ceil
         cur = prev;
     }
     return x;
