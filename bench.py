@@ -44,7 +44,13 @@ SQ_PER_MODMUL = 3  # INT32 multiplies per modular multiplication (reference coun
 METRIC = "MR base-2 tests/s, uniform batch of 256 x 50 000-digit candidates, served/batched"
 WORKLOAD = ("uniform MR batch: 256 x 50 000-digit N/rev(N), (k,j) from the (50000,30000,100) sieve "
             "survivors, splitmix64 seed 1")
-PERSIST_LAUNCH_DRAM_BYTES = 517586944 + 219800832  # dram__bytes_read.sum + dram__bytes_write.sum
+# dram__bytes_read.sum + dram__bytes_write.sum of the timed persist_kernel launch of
+# the uniform batch (1024 squarings x 256 candidates, L2 flushed before it), from one
+# ncu capture of this build (profiles/persist_kernel_uniform_batch_dram.txt), in a run
+# whose autotuner chose 16-step quanta at L = 2^14: a run with longer quanta re-reads
+# the residues less often
+PERSIST_LAUNCH_DRAM_BYTES = 91944448 + 51434496
+PERSIST_LAUNCH_DRAM_QUANTUM = 16
 
 
 def ref_modmuls_per_squaring(digits: int) -> int:
@@ -615,10 +621,13 @@ def main():
     achieved = squarings / t_mr * ref_mults  # INT32 multiplies / s (one GPU)
     roofline = {"bound": "int32", "achieved": achieved / 1e12, "peak": peak_lo / 1e12, "unit": "Tmul/s",
                 "frac": achieved / peak_lo,
-                # DRAM bytes (read + write) of one timed launch of this workload (1024 squarings x
-                # 256 candidates, L2 flushed before it), from one ncu capture of the same command:
-                # profiles/persist_kernel_uniform_batch_dram.txt
+                # DRAM bytes (read + write) of one timed launch of this workload, from one ncu
+                # capture of this build (see PERSIST_LAUNCH_DRAM_BYTES); the quantum of that
+                # capture and this run's are both reported
                 "traffic": PERSIST_LAUNCH_DRAM_BYTES if chunk == 1024 and n == 256 else None,
+                "traffic_source": "ncu capture of this build's timed launch (profiles/"
+                                  "persist_kernel_uniform_batch_dram.txt), %d-step quanta" % PERSIST_LAUNCH_DRAM_QUANTUM,
+                "quantum": eng.tuning(14)[0],
                 "peak_source": "measured live: pfb_measure_int32_peak (mul.lo)",
                 "mul_hi_peak": peak_hi / 1e12,
                 "work": "%d INT32 multiplies per squaring (reference structure at %d digits)" % (ref_mults, digits)}
