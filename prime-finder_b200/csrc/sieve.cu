@@ -86,6 +86,31 @@ struct pfb_sieve {
 
 namespace {
 
+// The primes at or above the small limit: the medium kernel (a warp per
+// prime) below medium_limit, the large kernel (a thread per prime) above;
+// the digit count D of K is a template argument of both.
+template <int D>
+void enqueue_large_d(const uint32_t *primes, uint32_t n, uint32_t s_limit, const long long *abc, int n_abc,
+                     int K, uint32_t *mask, size_t wpt, int sms, cudaStream_t st) {
+    const uint32_t p_med = medium_limit(K, s_limit);
+    if (p_med > s_limit)
+        medium_kernel<D><<<dim3((unsigned)sms * 4u, (unsigned)n_abc), kBlockLarge, 0, st>>>(
+            primes, n, s_limit, p_med, abc, K, mask, wpt);
+    const unsigned blocks = (n + kBlockLarge - 1u) / kBlockLarge;
+    large_kernel<D><<<dim3(blocks, (unsigned)n_abc), kBlockLarge, 0, st>>>(primes, n, p_med, abc, K, mask, wpt);
+}
+
+cudaError_t enqueue_large(const uint32_t *primes, uint32_t n, uint32_t s_limit, const long long *abc, int n_abc,
+                          int K, uint32_t *mask, size_t wpt, int sms, cudaStream_t st) {
+    switch (ndigits(K)) {
+    case 1: enqueue_large_d<1>(primes, n, s_limit, abc, n_abc, K, mask, wpt, sms, st); break;
+    case 2: enqueue_large_d<2>(primes, n, s_limit, abc, n_abc, K, mask, wpt, sms, st); break;
+    case 3: enqueue_large_d<3>(primes, n, s_limit, abc, n_abc, K, mask, wpt, sms, st); break;
+    default: enqueue_large_d<4>(primes, n, s_limit, abc, n_abc, K, mask, wpt, sms, st); break;
+    }
+    return cudaGetLastError();
+}
+
 int ensure_split(pfb_sieve *s, int K) {
     const uint32_t lim = small_limit(K);
     if (lim == s->s_limit) return PFB_OK;
@@ -186,13 +211,9 @@ int enqueue_sieve(pfb_sieve *s, int n_abc, int K, uint32_t *d_mask, cudaStream_t
         small_tile_kernel<<<g2, kBlockTile, smem, st>>>(s->d_rec, s->d_counts, cap, K, d_mask, wpt);
         PFB_CUDA(cudaGetLastError());
     }
-    if (s->n_primes) {
-        int blocks = (int)((s->n_primes + kBlockLarge - 1) / kBlockLarge);
-        dim3 g3((unsigned)blocks, (unsigned)n_abc);
-        large_kernel<<<g3, kBlockLarge, 0, st>>>(s->d_primes, s->n_primes, s->s_limit, s->d_abc, K,
-                                                 d_mask, wpt);
-        PFB_CUDA(cudaGetLastError());
-    }
+    if (s->n_primes)
+        PFB_CUDA(enqueue_large(s->d_primes, s->n_primes, s->s_limit, s->d_abc, n_abc, K, d_mask, wpt,
+                               s->max_grid / 16, st));
     return PFB_OK;
 }
 
@@ -579,10 +600,7 @@ extern "C" int pfb_sieve_run_noalloc(const uint32_t *d_primes, uint32_t n_primes
         small_tile_kernel<<<dim3(tiles, 1u), kBlockTile, tile_smem_bytes(rows, K), st>>>(sc->rec, sc->counts,
                                                                                          2u * cap, K, d_mask, wpt);
         PFB_CUDA(cudaGetLastError());
-        const int lb = (int)((n_primes + kBlockLarge - 1) / kBlockLarge);
-        large_kernel<<<dim3((unsigned)lb, 1u), kBlockLarge, 0, st>>>(d_primes, n_primes, lim, sc->abc, K, d_mask,
-                                                                    wpt);
-        PFB_CUDA(cudaGetLastError());
+        PFB_CUDA(enqueue_large(d_primes, n_primes, lim, sc->abc, 1, K, d_mask, wpt, sms, st));
     }
     return PFB_OK;
 }

@@ -427,105 +427,158 @@ small_tile_kernel(const SmallRec *__restrict__ rec, const uint32_t *__restrict__
     }
 }
 
-// Large primes (p >= S > K): each line meets every row at most once.  One
-// thread per prime; incremental updates replace the multiplications.
+// Coefficients of the two lines of a large prime p (p >= S >= 10^D, D the
+// digit count of K; p prime, so 10 is invertible).
+//
+//   N form    j == an - k bn (mod p),  an = (10^a - 1) 10^-c,  bn = 10^(b-c)
+//   rev form  y == ar - x br (mod p),  ar = (10^a - 1) 10^(c+D-a),  br = 10^(c-b)
+//
+// The rev form of trial_div_cpu.c:54-101 has one congruence per digit class
+// (lk, lj) of (k, j): rev(j) == (10^a - 1) 10^(c+lj-a) - rev(k) 10^(c-b+lj-lk).
+// Multiplying it by 10^(D-lj) turns it into the single line above at
+// x = rev(k) 10^(D-lk), y = rev(j) 10^(D-lj): both below 10^D <= p, so the
+// scaled values are the residues themselves.  Conversely every point (x, y)
+// of the line with 1 <= x, y < 10^D is the point of exactly one class: x
+// written with D digits (leading zeros allowed) and reversed is k, whose
+// digit count is lk (k never starts with 0), likewise for y and j.  One
+// lattice walk over the 10^D - 1 values of x thus visits the hits of all
+// D x D classes.  The reference uses a class of lk digits only when
+// a - b - lk >= 0 (of lj digits: a - c - lj >= 0, trial_div_cpu.c:59-66,
+// 78-84), i.e. when k < 10^(a-b) (j < 10^(a-c)): class_max.
+struct LargeConsts {
+    uint32_t an, bn, ar, br;
+};
+
+__device__ void large_consts(const Mod32 &M, long long a, long long b, long long c, int D, LargeConsts &s) {
+    const uint32_t p = M.p;
+    const uint32_t d = p % 10u;
+    const uint32_t t = d == 1 ? 9u : d == 3 ? 3u : d == 7 ? 7u : 1u;
+    const uint32_t inv10 = (uint32_t)(((unsigned long long)p * t + 1ull) / 10ull);
+    // 10^e for any integer e
+    auto pw = [&](long long e) -> uint32_t {
+        return e >= 0 ? M.pow(10u, (unsigned long long)e) : M.pow(inv10, (unsigned long long)(-e));
+    };
+    const uint32_t ram1 = M.sub(pw(a), 1u);
+    s.an = M.mul(ram1, pw(-c));
+    s.bn = pw(b - c);
+    s.ar = M.mul(ram1, pw(c + D - a));
+    s.br = pw(c - b);
+}
+
+// Largest k (or j) of a class the reference uses, e = a - b (or a - c):
+// min(K, 10^min(e, D) - 1), 0 when no class is used.
+__device__ __forceinline__ uint32_t class_max(long long e, int D, int K) {
+    if (e < 1) return 0u;
+    const uint32_t m = pow10i(e < D ? (int)e : D) - 1u;
+    return m < (uint32_t)K ? m : (uint32_t)K;
+}
+
+// A prime of the large-prime kernels: at least the small limit and above
+// 10^D - 1, and coprime to 10 (anything else in the list is not a prime).
+__device__ __forceinline__ bool large_prime(uint32_t p, uint32_t lo, uint32_t hi, uint32_t X) {
+    return p >= lo && p < hi && p > X && (p & 1u) && p % 5u != 0u;
+}
+
+// Hits of one prime on x in [x0, x1] of both lines (x1 <= K on the N line,
+// <= X on the rev line; an empty range when x0 > x1).
+template <int D>
+__device__ __forceinline__ void large_lines(const Mod32 &M, const LargeConsts &lc, uint32_t nx0, uint32_t nx1,
+                                            uint32_t rx0, uint32_t rx1, uint32_t kmax, uint32_t jmax, int K,
+                                            uint32_t *m) {
+    constexpr uint32_t X = D == 1 ? 9u : D == 2 ? 99u : D == 3 ? 999u : 9999u;
+    if (nx0 <= nx1)  // N form (trial_div_cpu.c:40-52): at most one j per k
+        line_hits(M, lc.an, lc.bn, nx0, nx1, (uint32_t)K,
+                  [&](uint32_t k, uint32_t j) { mark_global(m, K, k, j); });
+    if (rx0 <= rx1 && kmax && jmax)
+        line_hits(M, lc.ar, lc.br, rx0, rx1, X, [&](uint32_t x, uint32_t y) {
+            const uint32_t k = rev_digits(x, D), j = rev_digits(y, D);
+            if (k <= kmax && j <= jmax) mark_global(m, K, k, j);
+        });
+}
+
+// Primes in [p_med, inf): one thread per prime, whole lines.  At most about
+// 2 K^2 / p_med hits per thread.
+template <int D>
 __global__ void __launch_bounds__(kBlockLarge)
-large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
+large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t p_med,
              const long long *__restrict__ abc, int K, uint32_t *__restrict__ mask,
              size_t words_per_triple) {
+    constexpr uint32_t X = D == 1 ? 9u : D == 2 ? 99u : D == 3 ? 999u : 9999u;
     const int t = blockIdx.y;
     const long long a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
     uint32_t *m = mask + (size_t)t * words_per_triple;
-    const int maxd = ndigits(K);
+    const uint32_t kmax = class_max(a - b, D, K), jmax = class_max(a - c, D, K);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t p = primes[i];
-        if (p < s_limit) continue;
+        if (!large_prime(p, p_med, 0xFFFFFFFFu, X)) continue;
         Mod32 M;
         M.init(p);
-        LineConsts lc;
-        line_consts(M, a, b, c, lc);
+        LargeConsts lc;
+        large_consts(M, a, b, c, D, lc);
+        large_lines<D>(M, lc, 1u, (uint32_t)K, 1u, X, kmax, jmax, K, m);
+    }
+}
 
-        if (lc.flags & 1u)  // N form: j == AN - k BN (p > K: at most one j per k)
-            line_hits(M, lc.an, lc.bn, 1u, (uint32_t)K, (uint32_t)K,
-                      [&](uint32_t k, uint32_t j) { mark_global(m, K, k, j); });
-        for (int lk = 1; lk <= maxd; lk++) {  // rev form, per digit class of k
-            if (!(lc.flags & (1u << lk))) continue;
-            const uint32_t lo = pow10i(lk - 1), hi = pow10i(lk) - 1u;
-            // State of the four j classes in registers.  A class that is off
-            // (no such digit count on the grid, or skipped by the reference's
-            // rules) keeps value 0 and step 0: 0 never passes the hit test.
-            uint32_t tv[4], st[4], on = 0u;
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                const bool c_on = (q + 1 <= maxd) && (lc.flags & (1u << (5 + q)));
-                on |= c_on ? (1u << q) : 0u;
-                st[q] = c_on ? lc.br[lk - 1][q] : 0u;
-                tv[q] = c_on ? lc.ar[q] : 0u;
-            }
-            if (hi <= (uint32_t)K && lk >= 3) {
-                // Long class (rev(k) takes up to 9999 values): per j class, a
-                // lattice walk when rev(j) has >= 3 digits; otherwise iterate
-                // the <= 99 values of rev(j): rev(k) == (AR - rev(j)) BR^-1,
-                // BR^-1 = 10^(b-c+lk-lj) = BN * 10^(lk-lj).  (Not unrolled:
-                // the walk is large and the instruction cache small.)
-#pragma unroll 1
-                for (int q = 0; q < 4; q++) {
-                    if (!(on & (1u << q))) continue;
-                    const int lj = q + 1;
-                    const uint32_t ylim = pow10i(lj) - 1u;
-                    if (lj >= 3) {
-                        line_hits(M, lc.ar[q], st[q], 1u, hi, ylim, [&](uint32_t rk, uint32_t rj) {
-                            if (rk % 10u != 0u && rj % 10u != 0u) {
-                                const uint32_t j = rev_digits(rj, lj);
-                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
-                            }
-                        });
-                    } else {
-                        const uint32_t inv = M.mul(lc.bn, pow10i(lk - lj) % p);
-                        uint32_t rk = M.mul(lc.ar[q], inv);  // rev(j) = 0
-                        for (uint32_t rj = 1; rj <= ylim; rj++) {
-                            rk = M.sub(rk, inv);
-                            if (rk - 1u < hi && rk % 10u != 0u && (lj == 1 || rj % 10u != 0u)) {
-                                const uint32_t j = rev_digits(rj, lj);
-                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
-                            }
-                        }
-                    }
-                }
-            } else if (hi <= (uint32_t)K) {
-                // short class (lk <= 2): walk rev(k) = 1 .. hi linearly
-#pragma unroll
-                for (int q = 0; q < 4; q++) tv[q] = M.sub(tv[q], st[q]);  // rk = 1
-                for (uint32_t rk = 1; rk <= hi; rk++) {
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (tv[q] - 1u < pow10i(q + 1) - 1u) {  // 1 <= rev(j) < 10^(q+1)
-                            const uint32_t rj = tv[q];
-                            if ((lk == 1 || rk % 10u != 0u) && (q == 0 || rj % 10u != 0u)) {
-                                const uint32_t j = rev_digits(rj, q + 1);
-                                if (j <= (uint32_t)K) mark_global(m, K, rev_digits(rk, lk), j);
-                            }
-                        }
-                        tv[q] = M.sub(tv[q], st[q]);
-                    }
-                }
-            } else {
-                // partial top class (K < 10^lk - 1): visit the k on the grid directly
-                for (uint32_t k = lo; k <= (uint32_t)K; k++) {
-                    const uint32_t rk = rev_digits(k, lk) % p;
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        if (!(on & (1u << q))) continue;
-                        const uint32_t rj = M.sub(lc.ar[q], M.mul(rk, st[q]));
-                        if (rj - 1u < pow10i(q + 1) - 1u && (q == 0 || rj % 10u != 0u)) {
-                            const uint32_t j = rev_digits(rj, q + 1);
-                            if (j <= (uint32_t)K) mark_global(m, K, k, j);
-                        }
-                    }
-                }
-            }
+// Primes in [s_limit, p_med), the ones with the most hits: a warp per
+// prime, lane l walking the l-th 32nd of each line's x range, so that no
+// single thread carries the ~2 K^2 / p hits of a small large prime.  Warp w
+// of W loads the list entries w + l W (lane l), then w + (32 + l) W, ...; on
+// a sorted list that hands every warp primes from across the whole range.
+// A lane that loaded a prime of the range sets up its lines, then the warp
+// walks the primes of the batch one after another, their constants
+// broadcast from the lane that holds them.
+template <int D>
+__global__ void __launch_bounds__(kBlockLarge)
+medium_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit, uint32_t p_med,
+              const long long *__restrict__ abc, int K, uint32_t *__restrict__ mask,
+              size_t words_per_triple) {
+    constexpr uint32_t X = D == 1 ? 9u : D == 2 ? 99u : D == 3 ? 999u : 9999u;
+    const int t = blockIdx.y;
+    const long long a = abc[3 * t], b = abc[3 * t + 1], c = abc[3 * t + 2];
+    uint32_t *m = mask + (size_t)t * words_per_triple;
+    const uint32_t kmax = class_max(a - b, D, K), jmax = class_max(a - c, D, K);
+    const uint32_t lane = threadIdx.x & 31u;
+    const size_t W = (size_t)gridDim.x * (blockDim.x >> 5);
+    const size_t w = (size_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const uint32_t nseg = ((uint32_t)K + 31u) / 32u, rseg = (X + 31u) / 32u;
+    const uint32_t nx0 = 1u + lane * nseg, rx0 = 1u + lane * rseg;
+    const uint32_t nx1 = min((uint32_t)K, nx0 + nseg - 1u), rx1 = min(X, rx0 + rseg - 1u);
+    for (size_t base = w; base < n; base += 32u * W) {
+        const size_t e = base + lane * W;
+        const uint32_t p = e < n ? primes[e] : 0u;
+        const bool mine = large_prime(p, s_limit, p_med, X);
+        unsigned todo = __ballot_sync(0xFFFFFFFFu, mine);
+        Mod32 M;
+        M.p = 0u;
+        M.m = 0ull;
+        LargeConsts lc{0u, 0u, 0u, 0u};
+        if (mine) {
+            M.init(p);
+            large_consts(M, a, b, c, D, lc);
+        }
+        while (todo) {
+            const int src = __ffs((int)todo) - 1;
+            todo &= todo - 1u;
+            Mod32 Ms;
+            Ms.p = __shfl_sync(0xFFFFFFFFu, M.p, src);
+            Ms.m = __shfl_sync(0xFFFFFFFFu, M.m, src);
+            LargeConsts ls;
+            ls.an = __shfl_sync(0xFFFFFFFFu, lc.an, src);
+            ls.bn = __shfl_sync(0xFFFFFFFFu, lc.bn, src);
+            ls.ar = __shfl_sync(0xFFFFFFFFu, lc.ar, src);
+            ls.br = __shfl_sync(0xFFFFFFFFu, lc.br, src);
+            large_lines<D>(Ms, ls, nx0, nx1, rx0, rx1, kmax, jmax, K, m);
         }
     }
+}
+
+// Bottom of the large-prime kernel's range: primes below it have more than
+// about 512 hits per thread and go to the medium kernel.
+inline uint32_t medium_limit(int K, uint32_t s_limit) {
+    const unsigned long long X = pow10i(ndigits(K)) - 1u;
+    const unsigned long long h = ((unsigned long long)K * (unsigned long long)K + X * X) / 512ull;
+    const uint32_t v = h < (1ull << 18) ? (uint32_t)h : (1u << 18);
+    return v > s_limit ? v : s_limit;
 }
 
 // Survivor compaction, pass 1: zero bits per 1024-bit chunk.

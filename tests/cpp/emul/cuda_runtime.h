@@ -320,6 +320,16 @@ inline T __shfl_xor_sync(unsigned, T v, int lane_mask) {
 }
 
 template <class T>
+inline T __shfl_sync(unsigned, T v, int src) {
+    const unsigned t = threadIdx.x, w = t >> 5;
+    (*emu::lane_vals)[t] = (unsigned long long)v;
+    emu::group_wait(1 + (int)w);
+    const T r = (T)(*emu::lane_vals)[(w << 5) + ((unsigned)src & 31u)];
+    emu::group_wait(1 + (int)w);
+    return r;
+}
+
+template <class T>
 inline T __shfl_up_sync(unsigned, T v, unsigned delta) {
     const unsigned t = threadIdx.x, w = t >> 5, lane = t & 31u;
     (*emu::lane_vals)[t] = (unsigned long long)v;

@@ -14,6 +14,7 @@
 #include <iostream>
 #include <sstream>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "sieve_device.cuh"
@@ -60,11 +61,27 @@ int main() {
             small_tile_kernel(rec.data(), counts.data(), 2u * cap, K, mask.data(), wpt);
         }, tile_smem_bytes(rows, K));
     }
-    // large primes: one thread per prime of the whole list
-    if (n)
-        emu::run_grid((n + kBlockLarge - 1) / kBlockLarge, 1, kBlockLarge, [&] {
-            large_kernel(primes.data(), n, lim, abc, K, mask.data(), wpt);
-        });
+    // medium primes (a warp per prime, a small grid so that the warps take
+    // several batches) and large primes (one thread per prime of the list)
+    const uint32_t p_med = medium_limit(K, lim);
+    if (n) {
+        auto large = [&](auto dc) {
+            constexpr int D = decltype(dc)::value;
+            if (p_med > lim)
+                emu::run_grid(2, 1, kBlockLarge, [&] {
+                    medium_kernel<D>(primes.data(), n, lim, p_med, abc, K, mask.data(), wpt);
+                });
+            emu::run_grid((n + kBlockLarge - 1) / kBlockLarge, 1, kBlockLarge, [&] {
+                large_kernel<D>(primes.data(), n, p_med, abc, K, mask.data(), wpt);
+            });
+        };
+        switch (ndigits(K)) {
+        case 1: large(std::integral_constant<int, 1>()); break;
+        case 2: large(std::integral_constant<int, 2>()); break;
+        case 3: large(std::integral_constant<int, 3>()); break;
+        default: large(std::integral_constant<int, 4>()); break;
+        }
+    }
     // survivor compaction (pfb_sieve_survivors)
     const uint32_t nbits = (uint32_t)K * (uint32_t)K, nwords = (nbits + 31u) / 32u, chunks = (nwords + 31u) / 32u;
     std::vector<uint32_t> chunk(chunks), out(compact ? nbits : 1);

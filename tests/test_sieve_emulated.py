@@ -96,6 +96,23 @@ def test_emulated_sieve_full_grid(emul):
     _check(*_run(emul, P, 50000, 30000, 100, 9999, compact=False)[:3], P, 50000, 30000, 100, 9999, compact=False)
 
 
+def test_emulated_sieve_medium_and_large_ranges(emul):
+    """Primes on both sides of the medium/large boundary (2^18 at K = 9999,
+    about 198 000 at K = 1200), in a shuffled list: the warp-per-prime kernel
+    below it, the thread-per-prime kernel above, every digit class of k and j
+    on one lattice walk per prime; triples with few classes in use
+    (a - b = 2, a - c = 3)."""
+    import random
+    P = primes_below(1_200_000)
+    pick = [int(p) for p in P[(P > 10_000) & (P < 10_400)]]
+    pick += [int(p) for p in P[(P > 197_000) & (P < 199_500)]]
+    pick += [int(p) for p in P[(P > 261_000) & (P < 264_000)]]
+    pick += [int(p) for p in P[(P > 1_190_000)]][:40]
+    random.Random(5).shuffle(pick)
+    for a, b, c, K in [(50000, 30000, 100, 9999), (50000, 30000, 100, 1200), (105, 103, 102, 1200)]:
+        _check(*_run(emul, pick, a, b, c, K, compact=False)[:3], pick, a, b, c, K, compact=False)
+
+
 def test_emulated_sieve_in_bounds(tmp_path):
     exe = str(tmp_path / "sieve_emul_asan")
     cc = _build(exe, asan=True)
