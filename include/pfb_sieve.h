@@ -106,7 +106,7 @@ int trial_div_gpu_grid(const uint32_t *primes, uint32_t n_primes,
  *   d_mask    device mask block of pfb_sieve_mask_bytes(K) bytes, written
  *             (or OR-ed with PFB_SIEVE_OR) asynchronously on `stream`
  * Limits: one triple per call, 1 <= K <= 9999 (PFB_E_CAPACITY otherwise).
- * Working memory is one fixed __device__ array of 1 081 976 bytes (1.08 MB)
+ * Working memory is one fixed __device__ array of 361 688 bytes (0.36 MB)
  * inside the library, held by every GPU that loads it until the process
  * exits; nothing is allocated.  All calls share that array: calls that
  * overlap on the GPU (two streams, two host threads) race and must be

@@ -201,14 +201,14 @@ int enqueue_sieve(pfb_sieve *s, int n_abc, int K, uint32_t *d_mask, cudaStream_t
             s->rec_bytes = need;
         }
         dim3 g1((n_small_all + 127u) / 128u, (unsigned)n_abc);
-        small_setup_kernel<<<g1, 128, 0, st>>>(s->d_tiny, s->d_small, s->d_counts, s->d_abc, n_abc, cap,
+        small_setup_kernel<<<g1, 128, 0, st>>>(s->d_tiny, s->d_small, s->d_counts, s->d_abc, n_abc, K, cap,
                                                s->d_rec);
         PFB_CUDA(cudaGetLastError());
         const uint32_t tiles = ((uint32_t)K + kTileRows - 1u) / kTileRows;
         const uint32_t max_rows = (uint32_t)K < (uint32_t)kTileRows ? (uint32_t)K : (uint32_t)kTileRows;
         const size_t smem = tile_smem_bytes(max_rows, K);
         dim3 g2(tiles, (unsigned)n_abc);
-        small_tile_kernel<<<g2, kBlockTile, smem, st>>>(s->d_rec, s->d_counts, cap, K, d_mask, wpt);
+        small_tile_kernel<<<g2, kBlockTile, smem, st>>>(s->d_rec, s->d_counts, cap, s->d_abc, K, d_mask, wpt);
         PFB_CUDA(cudaGetLastError());
     }
     if (s->n_primes)
@@ -517,8 +517,8 @@ struct NoAllocScratch {
     SmallRec rec[2 * kNoAllocListCap];
 };
 
-// 1 081 976 bytes (1.08 MB): the scratch of one triple at any K <= 9999.
-static_assert(sizeof(NoAllocScratch) == 1081976, "the size the header states");
+// 361 688 bytes (0.36 MB): the scratch of one triple at any K <= 9999.
+static_assert(sizeof(NoAllocScratch) == 361688, "the size the header states");
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
 
 // One block: clears the counts and the seen-bitmap, stores the triple.
@@ -593,12 +593,12 @@ extern "C" int pfb_sieve_run_noalloc(const uint32_t *d_primes, uint32_t n_primes
         PFB_CUDA(cudaGetLastError());
         // record stride 2*cap: tiny then small; the kernels read the counts on the device
         dim3 g1((2u * cap + 127u) / 128u, 1u);
-        small_setup_kernel<<<g1, 128, 0, st>>>(sc->tiny, sc->small, sc->counts, sc->abc, 1, 2u * cap, sc->rec);
+        small_setup_kernel<<<g1, 128, 0, st>>>(sc->tiny, sc->small, sc->counts, sc->abc, 1, K, 2u * cap, sc->rec);
         PFB_CUDA(cudaGetLastError());
         const uint32_t tiles = ((uint32_t)K + kTileRows - 1u) / kTileRows;
         const uint32_t rows = (uint32_t)K < (uint32_t)kTileRows ? (uint32_t)K : (uint32_t)kTileRows;
-        small_tile_kernel<<<dim3(tiles, 1u), kBlockTile, tile_smem_bytes(rows, K), st>>>(sc->rec, sc->counts,
-                                                                                         2u * cap, K, d_mask, wpt);
+        small_tile_kernel<<<dim3(tiles, 1u), kBlockTile, tile_smem_bytes(rows, K), st>>>(
+            sc->rec, sc->counts, 2u * cap, sc->abc, K, d_mask, wpt);
         PFB_CUDA(cudaGetLastError());
         PFB_CUDA(enqueue_large(d_primes, n_primes, lim, sc->abc, 1, K, d_mask, wpt, sms, st));
     }

@@ -43,6 +43,53 @@ inline uint32_t small_limit(int K) {
     return s > 4096u ? s : 4096u;
 }
 
+// Coefficients of the two lines of a prime p coprime to 10 (D the digit
+// count of K, X = 10^D - 1):
+//
+//   N form    j == an - k bn (mod p),  an = (10^a - 1) 10^-c,  bn = 10^(b-c)
+//   rev form  y == ar - x br (mod p),  ar = (10^a - 1) 10^(c+D-a),  br = 10^(c-b)
+//
+// The rev form of trial_div_cpu.c:54-101 has one congruence per digit class
+// (lk, lj) of (k, j): rev(j) == (10^a - 1) 10^(c+lj-a) - rev(k) 10^(c-b+lj-lk).
+// Multiplied by 10^(D-lj) it is the single congruence above at
+// x = rev(k) 10^(D-lk), y = rev(j) 10^(D-lj), both in [1, X]; as 10 is
+// invertible mod p the two are equivalent.  Conversely every solution (x, y)
+// in [1, X]^2 is the point of exactly one class: x written with D digits
+// (leading zeros allowed) and reversed is k, whose digit count is lk (k never
+// starts with 0), likewise for y and j.  One line over x, y in [1, X] thus
+// holds the hits of all D x D classes.  The reference uses a class of lk
+// digits only when a - b - lk >= 0 (of lj digits: a - c - lj >= 0,
+// trial_div_cpu.c:59-66, 78-84), i.e. when k < 10^(a-b) (j < 10^(a-c)):
+// class_max.  The N form is always used for such p (trial_div_cpu.c:40-52).
+struct LargeConsts {
+    uint32_t an, bn, ar, br;
+};
+
+__device__ void large_consts(const Mod32 &M, long long a, long long b, long long c, int D, LargeConsts &s) {
+    const uint32_t p = M.p;
+    const uint32_t d = p % 10u;
+    const uint32_t t = d == 1 ? 9u : d == 3 ? 3u : d == 7 ? 7u : 1u;
+    const uint32_t inv10 = (uint32_t)(((unsigned long long)p * t + 1ull) / 10ull);
+    const uint32_t ten = 10u % p;
+    // 10^e for any integer e
+    auto pw = [&](long long e) -> uint32_t {
+        return e >= 0 ? M.pow(ten, (unsigned long long)e) : M.pow(inv10, (unsigned long long)(-e));
+    };
+    const uint32_t ram1 = M.sub(pw(a), 1u % p);
+    s.an = M.mul(ram1, pw(-c));
+    s.bn = pw(b - c);
+    s.ar = M.mul(ram1, pw(c + D - a));
+    s.br = pw(c - b);
+}
+
+// Largest k (or j) of a class the reference uses, e = a - b (or a - c):
+// min(K, 10^min(e, D) - 1), 0 when no class is used.
+__device__ __forceinline__ uint32_t class_max(long long e, int D, int K) {
+    if (e < 1) return 0u;
+    const uint32_t m = pow10i(e < D ? (int)e : D) - 1u;
+    return m < (uint32_t)K ? m : (uint32_t)K;
+}
+
 // Per (prime, triple) line coefficients.  flags: bit 0 = N form active,
 // bit lk = rev k-class lk active (1..4), bit 4+lj = rev j-class lj active.
 struct LineConsts {
@@ -53,11 +100,15 @@ struct LineConsts {
 };
 
 // Small-prime record kept in global memory between the set-up kernel and
-// the tile kernel.
+// the tile kernel: p, its Barrett constant and the coefficients of its two
+// lines (large_consts).  legacy = 1 for a p that shares a factor with 10 (5,
+// and 2 when listed): the tile kernel then takes the reference's per-class
+// congruences (line_consts), which the one-line form cannot merge.
 struct SmallRec {
     uint32_t p;
     uint32_t m_lo, m_hi;
-    LineConsts lc;
+    uint32_t an, bn, ar, br;
+    uint32_t legacy;
 };
 
 __device__ void line_consts(const Mod32 &M, long long a, long long b, long long c, LineConsts &s) {
@@ -329,11 +380,12 @@ __global__ void split_unique_kernel(const uint32_t *__restrict__ primes, uint32_
 // cap = 2 * capacity of each list.
 __global__ void small_setup_kernel(const uint32_t *__restrict__ tiny, const uint32_t *__restrict__ small,
                                    const uint32_t *__restrict__ counts, const long long *__restrict__ abc,
-                                   int n_abc, uint32_t cap, SmallRec *__restrict__ rec) {
+                                   int n_abc, int K, uint32_t cap, SmallRec *__restrict__ rec) {
     const uint32_t n_tiny = min(counts[0], cap / 2u), n_small = min(counts[1], cap / 2u);
     const uint32_t n = n_tiny + n_small;
     const int t = blockIdx.y;
     if (t >= n_abc) return;
+    const int D = ndigits(K);
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t p = i < n_tiny ? tiny[i] : small[i - n_tiny];
         Mod32 M;
@@ -342,21 +394,57 @@ __global__ void small_setup_kernel(const uint32_t *__restrict__ tiny, const uint
         r.p = p;
         r.m_lo = (uint32_t)M.m;
         r.m_hi = (uint32_t)(M.m >> 32);
-        line_consts(M, abc[3 * t], abc[3 * t + 1], abc[3 * t + 2], r.lc);
+        r.legacy = (p % 2u == 0u || p % 5u == 0u) ? 1u : 0u;
+        LargeConsts lc{0u, 0u, 0u, 0u};
+        if (!r.legacy) large_consts(M, abc[3 * t], abc[3 * t + 1], abc[3 * t + 2], D, lc);
+        r.an = lc.an;
+        r.bn = lc.bn;
+        r.ar = lc.ar;
+        r.br = lc.br;
         rec[(size_t)t * cap + i] = r;
     }
 }
 
-// Marks of one (prime,row) item.  Lanes lane0, lane0+step, ... of the hit
-// sequences are handled by this thread (step = 32 for warp items, 1 for
-// thread items).
-__device__ __forceinline__ void small_item(const SmallRec &r, uint32_t k, int K, uint32_t lane0,
-                                           uint32_t step, uint32_t *tile, uint32_t bit_base) {
+// Marks of one (prime,row) item in the tile.  Lanes lane0, lane0+step, ...
+// of the hit sequences are handled by this thread (step = 32 for warp items,
+// 1 for thread items).  Row k: the N-form hits j == an - k bn (mod p), and
+// the rev-form hits y == ar - rev_D(k) br (mod p), y in [1, X], j = rev_D(y),
+// of the classes in use (k <= kmax, j <= jmax).
+template <int D>
+__device__ __forceinline__ void small_item(const SmallRec &r, uint32_t k, int K, uint32_t kmax, uint32_t jmax,
+                                           uint32_t lane0, uint32_t step, uint32_t *tile, uint32_t bit_base) {
+    constexpr uint32_t X = D == 1 ? 9u : D == 2 ? 99u : D == 3 ? 999u : 9999u;
     Mod32 M;
     M.p = r.p;
     M.m = ((unsigned long long)r.m_hi << 32) | r.m_lo;
     const uint32_t p = r.p;
-    const LineConsts &lc = r.lc;
+    const uint32_t row = (k - 1u) * (uint32_t)K - bit_base;
+    auto mark = [&](uint32_t j) {
+        const uint32_t q = row + (j - 1u);
+        atomicOr(tile + (q >> 5), 1u << (q & 31u));
+    };
+    uint32_t j0 = M.sub(r.an, M.mul(k % p, r.bn));
+    if (j0 == 0) j0 = p;
+    for (uint32_t j = j0 + lane0 * p; j <= (uint32_t)K; j += step * p) mark(j);
+    if (k > kmax) return;
+    uint32_t y0 = M.sub(r.ar, M.mul(rev_digits(k, D) % p, r.br));
+    if (y0 == 0) y0 = p;
+    for (uint32_t y = y0 + lane0 * p; y <= X; y += step * p) {
+        const uint32_t j = rev_digits(y, D);
+        if (j <= jmax) mark(j);
+    }
+}
+
+// The same for a p that shares a factor with 10, on the reference's
+// per-class congruences (line_consts).
+__device__ void small_item_legacy(const SmallRec &r, const long long *abc, uint32_t k, int K, uint32_t lane0,
+                                  uint32_t step, uint32_t *tile, uint32_t bit_base) {
+    Mod32 M;
+    M.p = r.p;
+    M.m = ((unsigned long long)r.m_hi << 32) | r.m_lo;
+    const uint32_t p = r.p;
+    LineConsts lc;
+    line_consts(M, abc[0], abc[1], abc[2], lc);
     auto mark = [&](uint32_t j) {
         const uint32_t q = (k - 1u) * (uint32_t)K + (j - 1u) - bit_base;
         atomicOr(tile + (q >> 5), 1u << (q & 31u));
@@ -387,10 +475,33 @@ __device__ __forceinline__ void small_item(const SmallRec &r, uint32_t k, int K,
     }
 }
 
+template <int D>
+__device__ __forceinline__ void small_rows(const SmallRec *rt, uint32_t n_tiny, uint32_t n_small,
+                                           const long long *abc, uint32_t k0, uint32_t rows, int K,
+                                           uint32_t *tile, uint32_t bit_base) {
+    const uint32_t kmax = class_max(abc[0] - abc[1], D, K), jmax = class_max(abc[0] - abc[2], D, K);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    // Tiny primes: one warp per (prime,row), lanes share the hits.
+    for (uint32_t it = warp; it < n_tiny * rows; it += nwarps) {
+        const SmallRec r = rt[it / rows];
+        const uint32_t k = k0 + it % rows;
+        if (r.legacy) small_item_legacy(r, abc, k, K, lane, 32u, tile, bit_base);
+        else small_item<D>(r, k, K, kmax, jmax, lane, 32u, tile, bit_base);
+    }
+    // Other small primes: one thread per (prime,row).
+    for (uint32_t it = threadIdx.x; it < n_small * rows; it += blockDim.x) {
+        const SmallRec r = rt[n_tiny + it / rows];
+        const uint32_t k = k0 + it % rows;
+        if (r.legacy) small_item_legacy(r, abc, k, K, 0u, 1u, tile, bit_base);
+        else small_item<D>(r, k, K, kmax, jmax, 0u, 1u, tile, bit_base);
+    }
+}
+
 // Row-tile sieve of the small primes.  grid = (tiles, triples).
 __global__ void __launch_bounds__(kBlockTile)
 small_tile_kernel(const SmallRec *__restrict__ rec, const uint32_t *__restrict__ counts, uint32_t cap,
-                  int K, uint32_t *__restrict__ mask, size_t words_per_triple) {
+                  const long long *__restrict__ abc, int K, uint32_t *__restrict__ mask,
+                  size_t words_per_triple) {
     PFB_DYNAMIC_SMEM(uint32_t, tile);
     const int t = blockIdx.y;
     const uint32_t k0 = 1u + blockIdx.x * kTileRows;
@@ -407,17 +518,12 @@ small_tile_kernel(const SmallRec *__restrict__ rec, const uint32_t *__restrict__
     const uint32_t n_tiny = min(counts[0], cap / 2u), n_small = min(counts[1], cap / 2u);
     const SmallRec *rt = rec + (size_t)t * cap;
     const uint32_t bit_base = w0 << 5;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-
-    // Tiny primes: one warp per (prime,row), lanes share the hits.
-    for (uint32_t it = warp; it < n_tiny * rows; it += nwarps) {
-        const SmallRec r = rt[it / rows];
-        small_item(r, k0 + it % rows, K, lane, 32u, tile, bit_base);
-    }
-    // Other small primes: one thread per (prime,row).
-    for (uint32_t it = threadIdx.x; it < n_small * rows; it += blockDim.x) {
-        const SmallRec r = rt[n_tiny + it / rows];
-        small_item(r, k0 + it % rows, K, 0u, 1u, tile, bit_base);
+    const long long *tabc = abc + 3 * t;
+    switch (ndigits(K)) {
+    case 1: small_rows<1>(rt, n_tiny, n_small, tabc, k0, rows, K, tile, bit_base); break;
+    case 2: small_rows<2>(rt, n_tiny, n_small, tabc, k0, rows, K, tile, bit_base); break;
+    case 3: small_rows<3>(rt, n_tiny, n_small, tabc, k0, rows, K, tile, bit_base); break;
+    default: small_rows<4>(rt, n_tiny, n_small, tabc, k0, rows, K, tile, bit_base); break;
     }
     __syncthreads();
     uint32_t *g = mask + (size_t)t * words_per_triple + w0;
@@ -425,52 +531,6 @@ small_tile_kernel(const SmallRec *__restrict__ rec, const uint32_t *__restrict__
         const uint32_t v = tile[w];
         if (v) atomicOr(g + w, v);
     }
-}
-
-// Coefficients of the two lines of a large prime p (p >= S >= 10^D, D the
-// digit count of K; p prime, so 10 is invertible).
-//
-//   N form    j == an - k bn (mod p),  an = (10^a - 1) 10^-c,  bn = 10^(b-c)
-//   rev form  y == ar - x br (mod p),  ar = (10^a - 1) 10^(c+D-a),  br = 10^(c-b)
-//
-// The rev form of trial_div_cpu.c:54-101 has one congruence per digit class
-// (lk, lj) of (k, j): rev(j) == (10^a - 1) 10^(c+lj-a) - rev(k) 10^(c-b+lj-lk).
-// Multiplying it by 10^(D-lj) turns it into the single line above at
-// x = rev(k) 10^(D-lk), y = rev(j) 10^(D-lj): both below 10^D <= p, so the
-// scaled values are the residues themselves.  Conversely every point (x, y)
-// of the line with 1 <= x, y < 10^D is the point of exactly one class: x
-// written with D digits (leading zeros allowed) and reversed is k, whose
-// digit count is lk (k never starts with 0), likewise for y and j.  One
-// lattice walk over the 10^D - 1 values of x thus visits the hits of all
-// D x D classes.  The reference uses a class of lk digits only when
-// a - b - lk >= 0 (of lj digits: a - c - lj >= 0, trial_div_cpu.c:59-66,
-// 78-84), i.e. when k < 10^(a-b) (j < 10^(a-c)): class_max.
-struct LargeConsts {
-    uint32_t an, bn, ar, br;
-};
-
-__device__ void large_consts(const Mod32 &M, long long a, long long b, long long c, int D, LargeConsts &s) {
-    const uint32_t p = M.p;
-    const uint32_t d = p % 10u;
-    const uint32_t t = d == 1 ? 9u : d == 3 ? 3u : d == 7 ? 7u : 1u;
-    const uint32_t inv10 = (uint32_t)(((unsigned long long)p * t + 1ull) / 10ull);
-    // 10^e for any integer e
-    auto pw = [&](long long e) -> uint32_t {
-        return e >= 0 ? M.pow(10u, (unsigned long long)e) : M.pow(inv10, (unsigned long long)(-e));
-    };
-    const uint32_t ram1 = M.sub(pw(a), 1u);
-    s.an = M.mul(ram1, pw(-c));
-    s.bn = pw(b - c);
-    s.ar = M.mul(ram1, pw(c + D - a));
-    s.br = pw(c - b);
-}
-
-// Largest k (or j) of a class the reference uses, e = a - b (or a - c):
-// min(K, 10^min(e, D) - 1), 0 when no class is used.
-__device__ __forceinline__ uint32_t class_max(long long e, int D, int K) {
-    if (e < 1) return 0u;
-    const uint32_t m = pow10i(e < D ? (int)e : D) - 1u;
-    return m < (uint32_t)K ? m : (uint32_t)K;
 }
 
 // A prime of the large-prime kernels: at least the small limit and above

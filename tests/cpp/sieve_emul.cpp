@@ -53,12 +53,12 @@ int main() {
     std::vector<SmallRec> rec(2 * cap);
     if (n_small_all) {
         emu::run_grid((n_small_all + 127u) / 128u, 1, 128, [&] {
-            small_setup_kernel(tiny.data(), small.data(), counts.data(), abc, 1, 2u * cap, rec.data());
+            small_setup_kernel(tiny.data(), small.data(), counts.data(), abc, 1, K, 2u * cap, rec.data());
         });
         const uint32_t tiles = ((uint32_t)K + kTileRows - 1u) / kTileRows;
         const uint32_t rows = (uint32_t)K < (uint32_t)kTileRows ? (uint32_t)K : (uint32_t)kTileRows;
         emu::run_grid(tiles, 1, kBlockTile, [&] {
-            small_tile_kernel(rec.data(), counts.data(), 2u * cap, K, mask.data(), wpt);
+            small_tile_kernel(rec.data(), counts.data(), 2u * cap, abc, K, mask.data(), wpt);
         }, tile_smem_bytes(rows, K));
     }
     // medium primes (a warp per prime, a small grid so that the warps take
