@@ -61,11 +61,11 @@ inline uint32_t small_limit(int K) {
 // digits only when a - b - lk >= 0 (of lj digits: a - c - lj >= 0,
 // trial_div_cpu.c:59-66, 78-84), i.e. when k < 10^(a-b) (j < 10^(a-c)):
 // class_max.  The N form is always used for such p (trial_div_cpu.c:40-52).
-struct LargeConsts {
+struct LineCoeffs {
     uint32_t an, bn, ar, br;
 };
 
-__device__ void large_consts(const Mod32 &M, long long a, long long b, long long c, int D, LargeConsts &s) {
+__device__ void line_coeffs(const Mod32 &M, long long a, long long b, long long c, int D, LineCoeffs &s) {
     const uint32_t p = M.p;
     const uint32_t d = p % 10u;
     const uint32_t t = d == 1 ? 9u : d == 3 ? 3u : d == 7 ? 7u : 1u;
@@ -101,7 +101,7 @@ struct LineConsts {
 
 // Small-prime record kept in global memory between the set-up kernel and
 // the tile kernel: p, its Barrett constant and the coefficients of its two
-// lines (large_consts).  legacy = 1 for a p that shares a factor with 10 (5,
+// lines (line_coeffs).  legacy = 1 for a p that shares a factor with 10 (5,
 // and 2 when listed): the tile kernel then takes the reference's per-class
 // congruences (line_consts), which the one-line form cannot merge.
 struct SmallRec {
@@ -310,19 +310,17 @@ __device__ __noinline__ FKBasis fk_reduce(uint32_t g, uint32_t p, uint32_t I) {
     return FKBasis{a, beta, c, delta};
 }
 
-// Calls visit(x, y) for every x in [x0, x1] with y = (A - B x) mod p in
-// [1, Y]; requires 1 <= Y < p, B != 0 (mod p), x1 - x0 < p.
-template <class Visit>
-__device__ __forceinline__ void line_hits(const Mod32 &M, uint32_t A, uint32_t B, uint32_t x0, uint32_t x1,
-                                          uint32_t Y, Visit visit) {
-    const uint32_t p = M.p;
-    const uint32_t g = p - B;
-    const uint32_t c0 = M.sub(M.sub(A, 1u % p), M.mul(B, x0 % p));  // (A - 1 - B x0) mod p
+// Calls visit(x0 + t, i + 1) for every t in [0, x1 - x0] with
+// i = (c0 + g t) mod p < Y; i_of(t) computes (c0 + g t) mod p.  Requires
+// 1 <= Y < p, g != 0, x1 - x0 < p.
+template <class IOf, class Visit>
+__device__ __forceinline__ void walk_hits(uint32_t c0, uint32_t g, uint32_t p, uint32_t x0, uint32_t x1, uint32_t Y,
+                                          IOf i_of, Visit visit) {
     unsigned long long t = first_hit(c0, g, p, Y);
     const unsigned long long span = (unsigned long long)(x1 - x0);
     if (t > span) return;
     const FKBasis fb = fk_reduce(g, p, Y);
-    uint32_t i = M.red((unsigned long long)g * t + c0);
+    uint32_t i = i_of((uint32_t)t);
     while (t <= span) {
         visit(x0 + (uint32_t)t, i + 1u);
         if (i >= fb.a) {
@@ -336,6 +334,45 @@ __device__ __forceinline__ void line_hits(const Mod32 &M, uint32_t A, uint32_t B
             t += (unsigned long long)fb.beta + fb.delta;
         }
     }
+}
+
+// Montgomery arithmetic for an odd modulus p < 2^32, R = 2^32: mul(a, b) =
+// a b R^-1 mod p for a, b < p.  m = lo(a b) p^-1 mod R makes a b - m p a
+// multiple of R, so the result is hi(a b) - hi(m p) (+ p): two mul.hi, two
+// mul.lo, no 64-bit sums.
+struct Mont32 {
+    uint32_t p, pinv;  // pinv = p^-1 mod 2^32
+
+    __device__ __forceinline__ void init(uint32_t p_) {
+        p = p_;
+        uint32_t x = p_;  // p x == 1 (mod 2^3) for odd p; each step doubles the bits
+        x *= 2u - p_ * x;
+        x *= 2u - p_ * x;
+        x *= 2u - p_ * x;
+        x *= 2u - p_ * x;
+        pinv = x;
+    }
+    __device__ __forceinline__ uint32_t mul(uint32_t a, uint32_t b) const {
+        const uint32_t hi = __umulhi(a, b), m = (a * b) * pinv, h = __umulhi(m, p);
+        return hi >= h ? hi - h : hi - h + p;
+    }
+    __device__ __forceinline__ uint32_t add(uint32_t a, uint32_t b) const {
+        const uint32_t s = a + b;
+        return (s < a || s >= p) ? s - p : s;
+    }
+    __device__ __forceinline__ uint32_t sub(uint32_t a, uint32_t b) const { return a >= b ? a - b : a - b + p; }
+};
+
+// Calls visit(x, y) for every x in [x0, x1] with y = (A - B x) mod p in
+// [1, Y]; requires 1 <= Y < p, B != 0 (mod p), x0 <= x1 < p.  Bm = B R mod
+// p: B x0 mod p is mul(Bm, x0) and g t mod p is mul(gm, t), so no 64-bit
+// value is reduced.
+template <class Visit>
+__device__ __forceinline__ void line_hits_m(const Mont32 &M, uint32_t A, uint32_t B, uint32_t Bm, uint32_t x0,
+                                            uint32_t x1, uint32_t Y, Visit visit) {
+    const uint32_t p = M.p, g = p - B, gm = p - Bm;
+    const uint32_t c0 = M.sub(M.sub(A, 1u), M.mul(Bm, x0));
+    walk_hits(c0, g, p, x0, x1, Y, [&](uint32_t t) { return M.add(M.mul(gm, t), c0); }, visit);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,8 +432,8 @@ __global__ void small_setup_kernel(const uint32_t *__restrict__ tiny, const uint
         r.m_lo = (uint32_t)M.m;
         r.m_hi = (uint32_t)(M.m >> 32);
         r.legacy = (p % 2u == 0u || p % 5u == 0u) ? 1u : 0u;
-        LargeConsts lc{0u, 0u, 0u, 0u};
-        if (!r.legacy) large_consts(M, abc[3 * t], abc[3 * t + 1], abc[3 * t + 2], D, lc);
+        LineCoeffs lc{0u, 0u, 0u, 0u};
+        if (!r.legacy) line_coeffs(M, abc[3 * t], abc[3 * t + 1], abc[3 * t + 2], D, lc);
         r.an = lc.an;
         r.bn = lc.bn;
         r.ar = lc.ar;
@@ -539,18 +576,66 @@ __device__ __forceinline__ bool large_prime(uint32_t p, uint32_t lo, uint32_t hi
     return p >= lo && p < hi && p > X && (p & 1u) && p % 5u != 0u;
 }
 
+// The line_coeffs coefficients, plain (an, bn, ar, br) and bn, br in
+// Montgomery form (bnm, brm).  The five powers 10^a, 10^-c, 10^(b-c),
+// 10^(c+D-a), 10^(c-b) come from one right-to-left binary exponentiation
+// over the exponents' bits: the squarings of 10 and of 10^-1 are shared,
+// each power multiplies in the square of its bits.  The exponents are the
+// triple's, the same in every thread, so the branches are uniform.
+struct LineCoeffsM {
+    uint32_t an, bn, ar, br, bnm, brm;
+};
+
+__device__ void line_coeffs_m(const Mont32 &M, long long a, long long b, long long c, int D, LineCoeffsM &s) {
+    const uint32_t p = M.p;
+    const uint32_t one = (0u - p) % p;  // R mod p
+    // 10 R mod p (doublings), R / 10 mod p = (R + k p) / 10 with R + k p == 0 (mod 10)
+    const uint32_t r2 = M.add(one, one), r4 = M.add(r2, r2), r8 = M.add(r4, r4);
+    uint32_t x10 = M.add(r8, r2);
+    const uint32_t pd = p % 10u, pi = pd == 1 ? 1u : pd == 3 ? 7u : pd == 7 ? 3u : 9u;  // p^-1 mod 10
+    const uint32_t k = ((10u - one % 10u) % 10u) * pi % 10u;
+    uint32_t xi = (uint32_t)(((unsigned long long)one + (unsigned long long)k * p) / 10ull);
+    const long long e[5] = {a, -c, b - c, c + D - a, c - b};
+    unsigned long long m[5];
+    uint32_t acc[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        m[q] = (unsigned long long)(e[q] < 0 ? -e[q] : e[q]);
+        acc[q] = one;
+    }
+    for (;;) {
+        bool more = false;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            if (m[q] & 1ull) acc[q] = M.mul(acc[q], e[q] < 0 ? xi : x10);
+            m[q] >>= 1;
+            more |= m[q] != 0ull;
+        }
+        if (!more) break;
+        x10 = M.mul(x10, x10);
+        xi = M.mul(xi, xi);
+    }
+    const uint32_t ram1 = M.sub(acc[0], one);  // (10^a - 1) R
+    s.bnm = acc[2];
+    s.brm = acc[4];
+    s.an = M.mul(M.mul(ram1, acc[1]), 1u);
+    s.bn = M.mul(acc[2], 1u);
+    s.ar = M.mul(M.mul(ram1, acc[3]), 1u);
+    s.br = M.mul(acc[4], 1u);
+}
+
 // Hits of one prime on x in [x0, x1] of both lines (x1 <= K on the N line,
 // <= X on the rev line; an empty range when x0 > x1).
 template <int D>
-__device__ __forceinline__ void large_lines(const Mod32 &M, const LargeConsts &lc, uint32_t nx0, uint32_t nx1,
+__device__ __forceinline__ void large_lines(const Mont32 &M, const LineCoeffsM &lc, uint32_t nx0, uint32_t nx1,
                                             uint32_t rx0, uint32_t rx1, uint32_t kmax, uint32_t jmax, int K,
                                             uint32_t *m) {
     constexpr uint32_t X = D == 1 ? 9u : D == 2 ? 99u : D == 3 ? 999u : 9999u;
     if (nx0 <= nx1)  // N form (trial_div_cpu.c:40-52): at most one j per k
-        line_hits(M, lc.an, lc.bn, nx0, nx1, (uint32_t)K,
-                  [&](uint32_t k, uint32_t j) { mark_global(m, K, k, j); });
+        line_hits_m(M, lc.an, lc.bn, lc.bnm, nx0, nx1, (uint32_t)K,
+                    [&](uint32_t k, uint32_t j) { mark_global(m, K, k, j); });
     if (rx0 <= rx1 && kmax && jmax)
-        line_hits(M, lc.ar, lc.br, rx0, rx1, X, [&](uint32_t x, uint32_t y) {
+        line_hits_m(M, lc.ar, lc.br, lc.brm, rx0, rx1, X, [&](uint32_t x, uint32_t y) {
             const uint32_t k = rev_digits(x, D), j = rev_digits(y, D);
             if (k <= kmax && j <= jmax) mark_global(m, K, k, j);
         });
@@ -571,10 +656,10 @@ large_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t p_med,
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t p = primes[i];
         if (!large_prime(p, p_med, 0xFFFFFFFFu, X)) continue;
-        Mod32 M;
+        Mont32 M;
         M.init(p);
-        LargeConsts lc;
-        large_consts(M, a, b, c, D, lc);
+        LineCoeffsM lc;
+        line_coeffs_m(M, a, b, c, D, lc);
         large_lines<D>(M, lc, 1u, (uint32_t)K, 1u, X, kmax, jmax, K, m);
     }
 }
@@ -608,25 +693,27 @@ medium_kernel(const uint32_t *__restrict__ primes, uint32_t n, uint32_t s_limit,
         const uint32_t p = e < n ? primes[e] : 0u;
         const bool mine = large_prime(p, s_limit, p_med, X);
         unsigned todo = __ballot_sync(0xFFFFFFFFu, mine);
-        Mod32 M;
+        Mont32 M;
         M.p = 0u;
-        M.m = 0ull;
-        LargeConsts lc{0u, 0u, 0u, 0u};
+        M.pinv = 0u;
+        LineCoeffsM lc{0u, 0u, 0u, 0u, 0u, 0u};
         if (mine) {
             M.init(p);
-            large_consts(M, a, b, c, D, lc);
+            line_coeffs_m(M, a, b, c, D, lc);
         }
         while (todo) {
             const int src = __ffs((int)todo) - 1;
             todo &= todo - 1u;
-            Mod32 Ms;
+            Mont32 Ms;
             Ms.p = __shfl_sync(0xFFFFFFFFu, M.p, src);
-            Ms.m = __shfl_sync(0xFFFFFFFFu, M.m, src);
-            LargeConsts ls;
+            Ms.pinv = __shfl_sync(0xFFFFFFFFu, M.pinv, src);
+            LineCoeffsM ls;
             ls.an = __shfl_sync(0xFFFFFFFFu, lc.an, src);
             ls.bn = __shfl_sync(0xFFFFFFFFu, lc.bn, src);
             ls.ar = __shfl_sync(0xFFFFFFFFu, lc.ar, src);
             ls.br = __shfl_sync(0xFFFFFFFFu, lc.br, src);
+            ls.bnm = __shfl_sync(0xFFFFFFFFu, lc.bnm, src);
+            ls.brm = __shfl_sync(0xFFFFFFFFu, lc.brm, src);
             large_lines<D>(Ms, ls, nx0, nx1, rx0, rx1, kmax, jmax, K, m);
         }
     }

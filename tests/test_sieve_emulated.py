@@ -101,16 +101,33 @@ def test_emulated_sieve_medium_and_large_ranges(emul):
     about 198 000 at K = 1200), in a shuffled list: the warp-per-prime kernel
     below it, the thread-per-prime kernel above, every digit class of k and j
     on one lattice walk per prime; triples with few classes in use
-    (a - b = 2, a - c = 3)."""
+    (a - b = 2, a - c = 3).  Four primes near 2^31 and 2^32 check the
+    Montgomery products at the top of the 32-bit range."""
     import random
     P = primes_below(1_200_000)
     pick = [int(p) for p in P[(P > 10_000) & (P < 10_400)]]
     pick += [int(p) for p in P[(P > 197_000) & (P < 199_500)]]
     pick += [int(p) for p in P[(P > 261_000) & (P < 264_000)]]
     pick += [int(p) for p in P[(P > 1_190_000)]][:40]
+    pick += [2147483629, 2147483647, 4294967279, 4294967291]  # near 2^31 and 2^32
     random.Random(5).shuffle(pick)
     for a, b, c, K in [(50000, 30000, 100, 9999), (50000, 30000, 100, 1200), (105, 103, 102, 1200)]:
         _check(*_run(emul, pick, a, b, c, K, compact=False)[:3], pick, a, b, c, K, compact=False)
+
+
+def test_line_coefficients_montgomery_and_barrett(tmp_path):
+    """The large kernels' coefficients (Montgomery products on shared squaring
+    chains of 10 and 10^-1) equal the small-prime set-up's (Barrett powers)
+    and 128-bit powers, for primes up to just below 2^32 and exponents of
+    either sign (tests/cpp/sieve_coeffs_check.cpp)."""
+    exe = str(tmp_path / "coeffs")
+    cc = subprocess.run(["g++", "-O2", "-std=c++20", "-Wno-unknown-pragmas"] + INC +
+                        [os.path.join(ROOT, "tests", "cpp", "sieve_coeffs_check.cpp"), "-o", exe],
+                        capture_output=True, text=True)
+    assert cc.returncode == 0, cc.stderr
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0 and r.stdout.startswith("ok "), r.stdout + r.stderr
+    assert int(r.stdout.split()[1]) >= 200 * 30 * 4
 
 
 def test_emulated_sieve_in_bounds(tmp_path):
