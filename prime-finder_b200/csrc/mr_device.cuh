@@ -123,24 +123,27 @@ __device__ __forceinline__ void load_tw(const uint32_t *__restrict__ W, const ui
 // j0 (all passes but the widest) its twiddles are loaded once per pass.
 
 // ZHI: the group's upper half (e >= R/2) is known to be zero and is not read;
-// the lower half holds limbs (< 2p), so the first stage is x, x w.
+// the lower half holds limbs (< 2p), so the first stage is x, x w.  The lower
+// half is read from src when given (same padded layout), else from A.
 // TSH > 0: the elements are first twisted for a negacyclic transform,
 // element i multiplied by psi^i = ww[i << (TSH - 1)] (Shoup companion wwsh).
 template <int PR, int RLOG, int SUB, bool ZHI = false, int TSH = 0>
 __device__ __forceinline__ void dif_group_t(uint32_t *__restrict__ A, int base, const uint32_t *tw,
                                             const uint32_t *tws, const uint32_t *__restrict__ ww = nullptr,
-                                            const uint32_t *__restrict__ wwsh = nullptr) {
+                                            const uint32_t *__restrict__ wwsh = nullptr,
+                                            const uint32_t *src = nullptr) {
     constexpr int R = 1 << RLOG, NL = ZHI ? R / 2 : R;
     constexpr uint32_t p = PR ? P2 : P1, p2 = 2u * p;
+    const uint32_t *in = (ZHI && src) ? src : A;
     uint32_t v[R];
     if constexpr (SUB % 32 == 0) {
         constexpr int PS = SUB + SUB / 32;  // pad(base + e SUB) = pad(base) + e PS
         const int pb = pad(base);
 #pragma unroll
-        for (int e = 0; e < NL; e++) v[e] = A[pb + e * PS];
+        for (int e = 0; e < NL; e++) v[e] = in[pb + e * PS];
     } else {
 #pragma unroll
-        for (int e = 0; e < NL; e++) v[e] = A[pad(base + e * SUB)];
+        for (int e = 0; e < NL; e++) v[e] = in[pad(base + e * SUB)];
     }
     if constexpr (TSH > 0) {
 #pragma unroll
@@ -229,7 +232,8 @@ template <int PR, int RLOG, int LOGN, int LH0, int STRIDE, bool ZHI = false, int
 __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint32_t *__restrict__ W,
                                            const uint32_t *__restrict__ Wsh, int g0,
                                            const uint32_t *__restrict__ ww = nullptr,
-                                           const uint32_t *__restrict__ wwsh = nullptr) {
+                                           const uint32_t *__restrict__ wwsh = nullptr,
+                                           const uint32_t *src = nullptr) {
     constexpr int R = 1 << RLOG, H0 = 1 << LH0;
     constexpr int GROUPS = (1 << LOGN) >> RLOG;
     constexpr int SUB = (2 * H0) >> RLOG;
@@ -240,7 +244,7 @@ __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint3
 #pragma unroll 1
         for (int gg = g0; gg < GROUPS; gg += STRIDE) {
             const int block = gg / SUB, j0 = gg % SUB;
-            dif_group_t<PR, RLOG, SUB, ZHI, TSH>(A, block * 2 * H0 + j0, ta, tsa, ww, wwsh);
+            dif_group_t<PR, RLOG, SUB, ZHI, TSH>(A, block * 2 * H0 + j0, ta, tsa, ww, wwsh, src);
         }
     } else {
 #pragma unroll 1
@@ -248,7 +252,7 @@ __device__ __forceinline__ void dif_pass_t(uint32_t *__restrict__ A, const uint3
             const int block = gg / SUB, j0 = gg % SUB;
             if constexpr (RLOG == 4) load_wide<0, PR>(LH0, j0, ta, tsa);
             else load_tw<RLOG, false>(W, Wsh, j0, SUB, LH0, ta, tsa);
-            dif_group_t<PR, RLOG, SUB, ZHI, TSH>(A, block * 2 * H0 + j0, ta, tsa, ww, wwsh);
+            dif_group_t<PR, RLOG, SUB, ZHI, TSH>(A, block * 2 * H0 + j0, ta, tsa, ww, wwsh, src);
         }
     }
 }
@@ -287,7 +291,8 @@ __device__ __forceinline__ void dit_pass_t(uint32_t *__restrict__ A, const uint3
 // negacyclic transform, the first pass twisting its inputs by psi^i (psi a
 // primitive 2^(LOGN+1)-th root of unity).
 template <bool TWO, int PR, int LOGN, int S, int STOP = 0, bool ZHI = false, bool NEG = false>
-__device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw) {
+__device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw,
+                                         const uint32_t *src = nullptr) {
     static_assert(!ZHI || (S == LOGN && S >= 4), "ZHI: first radix-16 pass of the transform");
     static_assert(!NEG || (S == LOGN && S > STOP && LOGN < LOG_LMAX), "NEG: a forward pass to twist in");
     if constexpr (S > STOP) {
@@ -297,13 +302,13 @@ __device__ __forceinline__ void dif_from(uint32_t *A0, uint32_t *A1, const Twidd
             constexpr int half = THREADS / 2;
             if ((int)threadIdx.x < half)
                 dif_pass_t<0, RLOG, LOGN, S - 1, half, ZHI, TSH>(A0, tw.w[0], tw.wsh[0], threadIdx.x, tw.w[0],
-                                                                  tw.wsh[0]);
+                                                                  tw.wsh[0], src);
             else
                 dif_pass_t<1, RLOG, LOGN, S - 1, half, ZHI, TSH>(A1, tw.w[1], tw.wsh[1], threadIdx.x - half, tw.w[1],
-                                                                  tw.wsh[1]);
+                                                                  tw.wsh[1], src);
         } else {
             dif_pass_t<PR, RLOG, LOGN, S - 1, THREADS, ZHI, TSH>(A0, tw.w[PR], tw.wsh[PR], threadIdx.x, tw.w[PR],
-                                                                  tw.wsh[PR]);
+                                                                  tw.wsh[PR], src);
         }
         __syncthreads();
         dif_from<TWO, PR, LOGN, S - RLOG, STOP>(A0, A1, tw);
@@ -409,9 +414,10 @@ __device__ __forceinline__ void mid_pass_t(uint32_t *__restrict__ A, const Twidd
 // inverse pass; needs at least one pass on each side of the middle sweep).
 template <bool TWO, int PR, int LOGN, int OP, bool CG, bool ZHI = false, bool NEG = false>
 __device__ __forceinline__ void product_from(uint32_t *A0, uint32_t *A1, const Twiddles &tw, const uint32_t *C0,
-                                             const uint32_t *C1, const CrtConsts &cc) {
+                                             const uint32_t *C1, const CrtConsts &cc,
+                                             const uint32_t *src = nullptr) {
     constexpr int M = mid_rlog<LOGN>();
-    dif_from<TWO, PR, LOGN, LOGN, M, ZHI, NEG>(A0, A1, tw);
+    dif_from<TWO, PR, LOGN, LOGN, M, ZHI, NEG>(A0, A1, tw, src);
     if constexpr (TWO) {
         constexpr int half = THREADS / 2;
         if ((int)threadIdx.x < half) mid_pass_t<0, LOGN, OP, CG, half>(A0, tw, C0, threadIdx.x, cc);
@@ -476,16 +482,16 @@ __device__ void dit1(uint32_t *A, int logn, const Twiddles &tw) {
 // Scratch of the carry-lookahead scan.
 struct CarrySmem {
     unsigned long long wc[THREADS / 32];
-    uint32_t wg[THREADS / 32], wp[THREADS / 32], wcin[THREADS / 32];
-    unsigned long long total;
-    unsigned long long aux[4];
+    uint32_t wg[THREADS / 32], wp[THREADS / 32];
+    uint32_t flag;
 };
 
 // Turns n raw coefficients get(i) (each < 2^63 - 2^42) plus a carry cin0 at
 // position 0 into n limbs of 22 bits written to out[] (padded index when
-// PAD), and returns the carry out of position n-1.  Each thread propagates a
-// segment of n/T consecutive positions; the carries between segments are
-// resolved by a generate/propagate scan (warp ballots, then across warps).
+// PAD), and returns the carry out of position n-1 (n >= 128, a power of
+// two).  Each thread propagates a segment of n/T consecutive positions; the
+// carries between segments are resolved by a generate/propagate scan (warp
+// ballots, then every warp over the warp aggregates): three block barriers.
 template <bool PAD, class Get>
 __device__ __forceinline__ unsigned long long carry_pass(const int n, const unsigned long long cin0, Get get,
                                                          uint32_t *out, CarrySmem &cs) {
@@ -531,16 +537,14 @@ __device__ __forceinline__ unsigned long long carry_pass(const int n, const unsi
         cs.wp[warp] = o1 & (o0 ^ 1u);
     }
     __syncthreads();
-    if (warp == 0) {
-        const int nw = (T + 31) >> 5;
-        const uint32_t G2 = __ballot_sync(FULL, lane < nw && cs.wg[lane]);
-        const uint32_t P2m = __ballot_sync(FULL, lane < nw && cs.wp[lane]);
-        const uint32_t X2 = (uint32_t)((unsigned long long)G2 + (unsigned long long)(G2 | P2m));
-        const uint32_t cinw = X2 ^ P2m;
-        if (lane < nw) cs.wcin[lane] = (cinw >> lane) & 1u;
-    }
-    __syncthreads();
-    const uint32_t X = (uint32_t)((unsigned long long)g + gp + cs.wcin[warp]);
+    // Every warp scans the warp aggregates itself: bit v of cw is the carry
+    // into warp v (v <= nw: the carry out of the last warp is bit nw).
+    constexpr int nw = T / 32;
+    static_assert(nw < 32, "one ballot holds the warp aggregates");
+    const uint32_t G2 = __ballot_sync(FULL, lane < nw && cs.wg[lane]);
+    const uint32_t P2m = __ballot_sync(FULL, lane < nw && cs.wp[lane]);
+    const uint32_t cw = (uint32_t)((unsigned long long)G2 + (unsigned long long)(G2 | P2m)) ^ P2m;
+    const uint32_t X = (uint32_t)((unsigned long long)g + gp + ((cw >> warp) & 1u));
     const uint32_t dprev = ((X ^ p) >> lane) & 1u;
     const unsigned long long cin = prev + dprev;
     if (t < na && cin) {
@@ -553,9 +557,10 @@ __device__ __forceinline__ unsigned long long carry_pass(const int n, const unsi
             a2 >>= LIMB_BITS;
         }
     }
-    if (t == na - 1) cs.total = acc + ((G || (Pr && dprev)) ? 1ull : 0ull);
-    __syncthreads();
-    const unsigned long long tot = cs.total;
+    // na is a multiple of 32 (n >= 64, a power of two): the last segment is
+    // lane 31 of warp na/32 - 1, its carry-out the carry into warp na/32.
+    const int wl = na >> 5;
+    const unsigned long long tot = cs.wc[wl - 1] + ((cw >> wl) & 1u);
     __syncthreads();
     return tot;
 }
@@ -665,6 +670,31 @@ __device__ __forceinline__ unsigned long long crt_signed(uint32_t r1, uint32_t r
 // length-L product).
 // On entry X, Y < c N with R' > 4 c^2 N (c = 4 for the strong test), or
 // X < R' for a plain REDC; on exit X < 2N * a.  A0 and A1 are clobbered.
+// X <- X + c mod B^H - 1 for the end-around carry c < 2^44 of a carry pass:
+// warp 0 adds c to limbs 0..31 with a ballot carry-lookahead; only when the
+// sum carries out of limb 31 (limbs 2..31 all B - 1) do full carry passes
+// take over.
+__device__ __forceinline__ void end_around(uint32_t *X, unsigned long long c, int H, CarrySmem &cs) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid < 32) {
+        const uint32_t add = lane == 0 ? (uint32_t)c & LIMB_MASK : (lane == 1 ? (uint32_t)(c >> LIMB_BITS) : 0u);
+        const uint32_t a = X[pad(lane)] + add;                  // < 2^23
+        const uint32_t limb = a & LIMB_MASK;
+        const uint32_t g = __ballot_sync(0xffffffffu, a > LIMB_MASK);
+        const uint32_t p = __ballot_sync(0xffffffffu, a <= LIMB_MASK && limb == LIMB_MASK);
+        const unsigned long long sum = (unsigned long long)g + (g | p);
+        const uint32_t cin = (((uint32_t)sum ^ p) >> lane) & 1u;  // carry into this limb
+        const bool over = (sum >> 32) != 0ull;                    // out of limb 31
+        if (!over) X[pad(lane)] = (limb + cin) & LIMB_MASK;
+        if (lane == 0) cs.flag = over ? 1u : 0u;
+    }
+    __syncthreads();
+    if (cs.flag) {
+        __syncthreads();
+        while (c) c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
+    }
+}
+
 template <bool MUL, int LOGL>
 __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t a, const Twiddles &tw,
                           const CrtConsts &cc, const uint32_t *gy = nullptr) {
@@ -680,14 +710,9 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
     unsigned long long cS = 0;
     if constexpr (FULL) {
         if (prod) {
-            for (int i = tid; i < H; i += T) {
-                const uint32_t v = X[pad(i)];
-                A0[pad(i)] = v;
-                A1[pad(i)] = v;
-            }
-            __syncthreads();
-            if (MUL && gy) product_from<true, 0, LOGL, 1, true, true>(A0, A1, tw, gy, gy + L, cc);
-            else product_from<true, 0, LOGL, 0, false, true>(A0, A1, tw, nullptr, nullptr, cc);
+            // the first forward pass reads the H limbs from X itself
+            if (MUL && gy) product_from<true, 0, LOGL, 1, true, true>(A0, A1, tw, gy, gy + L, cc, X);
+            else product_from<true, 0, LOGL, 0, false, true>(A0, A1, tw, nullptr, nullptr, cc, X);
             carry_pass<true>(L, 0ull, [&](int i) { return crt(A0[pad(i)], A1[pad(i)], LOGL, cc); }, A0, cs);
             cS = carry_pass<true>(H, 0ull,
                                   [&](int i) { return (unsigned long long)A0[pad(i)] + A0[pad(i + H)]; }, X, cs);
@@ -746,33 +771,42 @@ __device__ void mont_step(const Smem &sm, const Cand &cd, bool square, uint32_t 
         return crt_signed(P[pad(i)], Q[pad(i)], LOGH, cc, i == 0 ? OFF_N0 : OFF_C);
     }, P, cs);
     // m = lo - cM, plus R' when lo < cM (lo: the H limbs in P); modulo
-    // B^H - 1 that is lo - cM + 2 neg
-    bool z = true;
-    for (int i = tid; i < H; i += T) z = z && (i < 2 || P[pad(i)] == 0u);
-    const bool upper_zero = __syncthreads_and(z) != 0;
-    const bool neg = upper_zero && ((((unsigned long long)P[pad(1)] << LIMB_BITS) | P[pad(0)]) < cM);
-    __syncthreads();
+    // B^H - 1 that is lo - cM + 2 neg.  lo < cM < 2^44 needs limbs 2.. zero:
+    // the fold records that, and only then is limb 0 corrected.
     {
         const uint32_t m0 = (uint32_t)cM & LIMB_MASK, m1 = (uint32_t)(cM >> LIMB_BITS);
+        bool z = true;
         for (int i = tid; i < H; i += T) {
-            const uint32_t v = P[pad(i)] + (i == 0 && neg ? 2u : 0u), c = i == 0 ? m0 : (i == 1 ? m1 : 0u);
+            const uint32_t v = P[pad(i)], c = i == 0 ? m0 : (i == 1 ? m1 : 0u);
+            z = z && (i < 2 || v == 0u);
             P[pad(i)] = v + P1 - c;
             Q[pad(i)] = v + P2 - c;
         }
-        __syncthreads();
+        if (__syncthreads_and(z)) {
+            if (tid == 0) {
+                const unsigned long long lo =
+                    ((unsigned long long)(P[pad(1)] - P1 + m1) << LIMB_BITS) | (P[pad(0)] - P1 + m0);
+                if (lo < cM) {
+                    P[pad(0)] += 2u;
+                    Q[pad(0)] += 2u;
+                }
+            }
+            __syncthreads();
+        }
     }
     // W = m N (mod B^H - 1) on (P, Q), then V = S + W into X; end-around carries
     product_from<true, 0, LOGH, 1, false>(P, Q, tw, cd.nh, cd.nh + H, cc);
     unsigned long long c = carry_pass<true>(H, cS, [&](int i) {
         return (unsigned long long)Sb[pad(i)] + crt_signed(P[pad(i)], Q[pad(i)], LOGH, cc, OFF_C);
     }, X, cs);
-    while (c) c = carry_pass<true>(H, c, [&](int i) { return (unsigned long long)X[pad(i)]; }, X, cs);
+    if (c) end_around(X, c, H, cs);
     // V = B^H - 1 represents 0 (U = 0: T = 0)
     bool ones = true;
     for (int i = tid; i < H; i += T) ones = ones && (X[pad(i)] == LIMB_MASK);
-    if (__syncthreads_and(ones))
+    if (__syncthreads_and(ones)) {
         for (int i = tid; i < H; i += T) X[pad(i)] = 0u;
-    __syncthreads();
+        __syncthreads();
+    }
     // X = a U from V = 2U
     if (a & 1u) {
         for (int i = tid; i < H; i += T) {

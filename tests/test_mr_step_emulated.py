@@ -134,3 +134,20 @@ def test_no_out_of_bounds_access(tmp_path):
     r = subprocess.run([exe], input="\n".join(lines) + "\n", capture_output=True, text=True, env=env, timeout=600)
     assert r.returncode == 0 and "ERROR: AddressSanitizer" not in r.stderr, r.stderr[-2000:]
     assert [int(v, 16) for v in r.stdout.split()] == want
+
+
+def test_carry_pass_and_end_around_carry(tmp_path):
+    """carry_pass (three block barriers, every warp scanning the warp
+    aggregates) and end_around (warp-0 ripple, full passes when the carry
+    runs past limb 31) against serial carries on the host, including limbs
+    of all B - 1 that make the carry run the whole length
+    (tests/cpp/carry_emul.cpp)."""
+    exe = str(tmp_path / "carry_emul")
+    subprocess.run(["g++", "-O2", "-std=c++20", "-Wno-unknown-pragmas",
+                    "-I", os.path.join(ROOT, "tests", "cpp", "emul"),
+                    "-I", os.path.join(ROOT, "prime-finder_b200", "csrc"),
+                    "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cpp", "carry_emul.cpp"), "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=900)
+    assert r.returncode == 0 and r.stdout.startswith("ok "), r.stdout + r.stderr
+    assert int(r.stdout.split()[1]) >= 9 * 6 + 8 * 4 * 7
