@@ -49,7 +49,7 @@ WORKLOAD = ("uniform MR batch: 256 x 50 000-digit N/rev(N), (k,j) from the (5000
 # ncu capture of this build (profiles/persist_kernel_uniform_batch_dram.txt), in a run
 # whose autotuner chose 16-step quanta at L = 2^14: a run with longer quanta re-reads
 # the residues less often
-PERSIST_LAUNCH_DRAM_BYTES = 91944448 + 51434496
+PERSIST_LAUNCH_DRAM_BYTES = 73122560 + 30478080
 PERSIST_LAUNCH_DRAM_QUANTUM = 16
 
 
