@@ -10,17 +10,18 @@
 //                pair of digit counts (lk, lj) of k and j.
 //    AN, BN, AR, BR are products of powers of 10 and 10^-1 mod p; 10^-1 mod p
 //    has a closed form, so no Fermat inversion is needed (the reference
-//    inverts with powmod(x, p-2, p), trial_div.cu:107).
+//    inverts with powmod(x, p-2, p), trial_div.cu:107).  For p coprime to
+//    10 the rev lines of all digit classes are one line, y == ar - x br, at
+//    x = rev_D(k), y = rev_D(j) (D = digits of K; sieve_device.cuh).
 //  * Small primes (p < S, S = max(4096, 10^digits(K))) hit many cells per row.
 //    They are sieved row-tile by row-tile in shared memory; primes below 512
 //    use one warp per (prime,row) so the 3333 hits of p = 3 in a row are
 //    spread over 32 lanes.  The finished tile is OR-ed into global memory
 //    with coalesced 32-bit atomics.
-//  * Large primes (p >= S) hit each row at most once.  One thread per prime
-//    enumerates the hits of its long lines with a lattice walk (O(log p) per
-//    line plus O(1) per hit), iterates the short lines (<= 99 values on one
-//    side) with incremental modular updates, and OR-s the hits into global
-//    memory.
+//  * Large primes (p >= S) hit each row at most once.  Their two lines are
+//    enumerated by lattice walks (O(log p) per line plus O(1) per hit): a
+//    warp per prime below 2^18 (lanes split the range of x), a thread per
+//    prime above; hits are OR-ed into global memory.
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdint.h>
