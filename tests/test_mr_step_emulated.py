@@ -89,6 +89,29 @@ def test_general_product_and_conversion(emul, logl):
     assert emul(lines) == want
 
 
+@pytest.mark.parametrize("logl", LENGTHS)
+def test_reduction_with_small_m(emul, logl):
+    """REDC of T = R' - k N has m = k exactly, and of T = j N has m = R' - j:
+    the step's m product returns limbs that are zero above the second, so the
+    fold's test for m = lo - cM < 0 decides the result; with T = j N it is
+    negative and R' is added.  k from 1 to past 2^44, j = 1, 2, 3."""
+    rng = random.Random(300 + logl)
+    R = (1 << (22 << (logl - 1))) + 1
+    lines, want = [], []
+    for _ in range(2):
+        N = modulus(rng, logl, 2)
+        for k in (1, 2, 3, 977, 1 << 21, (1 << 22) + 1, 1 << 43, (1 << 44) + 5, rng.getrandbits(40)):
+            T = R - k * N
+            if T <= 0:
+                continue
+            lines.append("redc %d %x %x" % (logl, N, T))
+            want.append(redc(logl, N, T))
+        for j in (1, 2, 3):
+            lines.append("redc %d %x %x" % (logl, N, j * N))
+            want.append(redc(logl, N, j * N))
+    assert emul(lines) == want
+
+
 def test_montgomery_ladder_equals_pow(emul):
     """A short square-and-multiply ladder in Montgomery form, fed back through
     the emulated step, ends at pow(2, e, N): the step composes as the
