@@ -544,7 +544,13 @@ def main():
     autotune = {"chosen": {str(k): {"quantum": v[0], "chunk": v[1]} for k, v in tune["chosen"].items()},
                 "tried": [[r["logl"], r["quantum"], r["chunk"], round(r["squarings_per_s_1"]),
                            round(r["squarings_per_s_2"])] for r in tune["tried"]],
-                "columns": "logl, quantum, chunk, squarings/s at 1 and at 2 candidates per SM"}
+                "columns": "logl, quantum, chunk, squarings/s at 1 and at 2 candidates per SM",
+                "fixed": {"lengths": "powers of two 2^8..2^15 (the NTT primes have no factor 3 in p - 1)",
+                          "radix": "16 (remainder pass 2, 4 or 8)",
+                          "product_form": "one length-L square up to 2^14, cyclic and negacyclic "
+                                          "halves at 2^15 (shared-memory capacity)",
+                          "candidates_per_cta": "1 (512 threads x 128 registers fill the register file)",
+                          "cluster": "1"}}
     batch = pfb200.MRBatch(eng, cands, 2)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device="cuda")
     chunk = args.chunk
