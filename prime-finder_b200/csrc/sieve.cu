@@ -20,8 +20,8 @@
 //    with coalesced 32-bit atomics.
 //  * Large primes (p >= S) hit each row at most once.  Their two lines are
 //    enumerated by lattice walks (O(log p) per line plus O(1) per hit): a
-//    warp per prime below 2^18 (lanes split the range of x), a thread per
-//    prime above; hits are OR-ed into global memory.
+//    warp per prime below (K^2 + X^2) / 12288 (lanes split the range of x),
+//    a thread per prime above; hits are OR-ed into global memory.
 #include <cuda_runtime.h>
 #include <stdarg.h>
 #include <stdint.h>

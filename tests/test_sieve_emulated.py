@@ -97,15 +97,16 @@ def test_emulated_sieve_full_grid(emul):
 
 
 def test_emulated_sieve_medium_and_large_ranges(emul):
-    """Primes on both sides of the medium/large boundary (2^18 at K = 9999,
-    about 198 000 at K = 1200), in a shuffled list: the warp-per-prime kernel
-    below it, the thread-per-prime kernel above, every digit class of k and j
-    on one lattice walk per prime; triples with few classes in use
-    (a - b = 2, a - c = 3).  Four primes near 2^31 and 2^32 check the
+    """Primes on both sides of the medium/large boundary (16 276 at K = 9999;
+    at K = 1200 every prime is above it), in a shuffled list: the
+    warp-per-prime kernel below it, the thread-per-prime kernel above, every
+    digit class of k and j on one lattice walk per prime; triples with few
+    classes in use (a - b = 2, a - c = 3).  Four primes near 2^31 and 2^32 check the
     Montgomery products at the top of the 32-bit range."""
     import random
     P = primes_below(1_200_000)
     pick = [int(p) for p in P[(P > 10_000) & (P < 10_400)]]
+    pick += [int(p) for p in P[(P > 16_000) & (P < 16_600)]]
     pick += [int(p) for p in P[(P > 197_000) & (P < 199_500)]]
     pick += [int(p) for p in P[(P > 261_000) & (P < 264_000)]]
     pick += [int(p) for p in P[(P > 1_190_000)]][:40]
